@@ -1,0 +1,169 @@
+/*
+ * ppf_b200 -- C ABI of the B200 point pair feature (PPF) registration engine.
+ *
+ * Drop-in boundary for the reference's registration path
+ * (nicolasavru/ppf-registration-spatial-hashing).  The reference exposes only
+ * C++ (include/ppf.h, include/model.h, include/scene.h); every entry point
+ * below names the reference interface it replaces.  Plain pointers and sizes,
+ * no C++ or framework types.  Nothing here exits the process or resets the
+ * device: failures return a status and ppf_last_error() describes them.
+ *
+ * Pointers: point/normal inputs may be host or device memory (detected per
+ * call).  Clouds are n x 3 float32 arrays (x, y, z per point), normals unit
+ * length.  Poses are 4x4 float32 row-major and map model coordinates into
+ * scene coordinates.
+ */
+#ifndef PPF_B200_H
+#define PPF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PPF_B200_ABI_VERSION 1
+
+typedef enum ppf_status {
+  PPF_OK = 0,
+  PPF_ERR_INVALID_ARGUMENT = 1, /* bad sizes, null pointers, out-of-range knobs */
+  PPF_ERR_CUDA = 2,             /* a CUDA runtime call failed */
+  PPF_ERR_OUT_OF_MEMORY = 3,    /* device allocation failed */
+  PPF_ERR_NO_VOTES = 4,         /* no scene pair matched the model: no pose */
+  PPF_ERR_TIMEOUT = 5,          /* a bounded device-side wait gave up */
+  PPF_ERR_INTERNAL = 6
+} ppf_status;
+#define PPF_ERR_OOM PPF_ERR_OUT_OF_MEMORY
+
+typedef struct ppf_context_s* ppf_context_t; /* device + stream + workspace */
+typedef struct ppf_model_s* ppf_model_t;     /* resident model hash array */
+typedef struct ppf_scene_s* ppf_scene_t;     /* resident scene cloud */
+
+/* Per-lookup statistics (the reference logs these at debug level,
+ * src/cuda/model.cu:122,152,161-168,280). */
+typedef struct ppf_stats {
+  uint64_t n_votes;          /* V: votes cast (sum of matched run lengths) */
+  uint64_t n_matched_pairs;  /* scene pairs whose key matched a model run */
+  uint32_t max_vote_count;   /* largest (s_r, m_r, alpha) vote count */
+  float min_votecount;       /* vote_count_threshold * max_vote_count */
+  uint64_t n_kept;           /* U: vote codes above the threshold */
+  uint64_t max_idx;          /* index of the chosen pose among the U */
+  float best_score;          /* its clustering score */
+  uint64_t n_candidates;     /* cells emitted by the vote pass (>= U) */
+  uint64_t n_exact_bins;     /* votes binned by the exact-atan2 path */
+  float vote_ms;             /* device time of the vote pass */
+  float total_ms;            /* device time of the whole lookup */
+  uint32_t gpu_launches;     /* kernels launched by the lookup */
+} ppf_stats;
+
+/* Error text of the last failing call on this thread ("" if none). */
+const char* ppf_last_error(void);
+int ppf_abi_version(void);
+
+/* Device selection as ppf_registration's devUse: device min(count-1, device)
+ * (src/cuda/ppf.cu:37-49).  The context owns a CUDA stream and a workspace;
+ * it never resets the device (the reference calls cudaDeviceReset at the end
+ * of ppf_registration, src/cuda/ppf.cu:103). */
+ppf_status ppf_context_create(int device, ppf_context_t* out);
+ppf_status ppf_context_destroy(ppf_context_t ctx);
+ppf_status ppf_context_synchronize(ppf_context_t ctx);
+/* The stream all work of this context is ordered on (a cudaStream_t). */
+void* ppf_context_stream(ppf_context_t ctx);
+/* Kernels this context has launched so far (running total). */
+uint64_t ppf_context_kernel_launches(ppf_context_t ctx);
+
+/* Model::Model(cloud, d_dist, vote_count_threshold, cpu_clustering,
+ * use_l1_norm, use_averaged_clusters) (include/model.h:17-19,
+ * src/cuda/model.cu:43-82): PPFs of all ordered model pairs, their keys and
+ * the sorted hash array, kept resident for any number of lookups.
+ * n must be in [2, 65535]. */
+ppf_status ppf_model_create(ppf_context_t ctx, const float* xyz, const float* nxyz, uint64_t n,
+                            float d_dist, float vote_count_threshold, int cpu_clustering,
+                            int use_l1_norm, int use_averaged_clusters, ppf_model_t* out);
+/* Model::SetModelPointVoteWeights (src/cuda/model.cu:91-93): n weights, one
+ * per model point (default 1.0); host or device pointer. */
+ppf_status ppf_model_set_point_vote_weights(ppf_model_t m, const float* w, uint64_t n);
+ppf_status ppf_model_destroy(ppf_model_t m);
+uint64_t ppf_model_num_points(ppf_model_t m);
+uint64_t ppf_model_num_keys(ppf_model_t m); /* unique feature keys K */
+
+/* Scene::Scene(cloud, d_dist, ref_point_downsample_factor)
+ * (include/scene.h:15-16, src/cuda/scene.cu:24-55).  Scene pair features are
+ * streamed during lookup, never materialised.  n must be >= 1 and < 2^31. */
+ppf_status ppf_scene_create(ppf_context_t ctx, const float* xyz, const float* nxyz, uint64_t n,
+                            float d_dist, uint32_t ref_point_df, ppf_scene_t* out);
+ppf_status ppf_scene_destroy(ppf_scene_t s);
+
+/* Model::ppf_lookup(scene) (src/cuda/model.cu:269-306) followed by the pose
+ * extraction of ppf_registration (src/cuda/ppf.cu:74-93): votes, threshold,
+ * poses, GPU pose clustering (or the greedy CPU clustering when the model was
+ * created with cpu_clustering) and the best pose, row-major into pose_out
+ * (host or device).  stats may be NULL.  The scene must have been created
+ * with the model's d_dist. */
+ppf_status ppf_model_lookup(ppf_model_t m, ppf_scene_t s, float* pose_out, ppf_stats* stats);
+
+/* ppf_registration(scene_clouds, model_clouds, model_d_dists,
+ * ref_point_downsample_factor, vote_count_threshold, cpu_clustering,
+ * use_l1_norm, use_averaged_clusters, devUse, model_weights)
+ * (include/ppf.h:9-15, src/cuda/ppf.cu:29-106): every scene against every
+ * model; poses_out receives n_scenes * n_models row-major 4x4 poses, indexed
+ * [scene][model] as the reference's result vector.  model_weights is accepted
+ * and ignored, as in the reference (src/cuda/ppf.cu:35); per-point weights go
+ * through ppf_model_set_point_vote_weights.  Each model's hash array is built
+ * once and reused for all scenes (the reference rebuilds it per scene with
+ * identical results).  A (scene, model) pair with no votes yields an all-zero
+ * pose and the call returns PPF_ERR_NO_VOTES after finishing the others. */
+ppf_status ppf_registration(ppf_context_t ctx, uint64_t n_scenes, const float* const* scene_xyz,
+                            const float* const* scene_nxyz, const uint64_t* scene_n,
+                            uint64_t n_models, const float* const* model_xyz,
+                            const float* const* model_nxyz, const uint64_t* model_n,
+                            const float* model_d_dists, uint32_t ref_point_df,
+                            float vote_count_threshold, int cpu_clustering, int use_l1_norm,
+                            int use_averaged_clusters, int dev_use, const float* model_weights,
+                            float* poses_out, ppf_stats* stats_out /* n_scenes*n_models or NULL */);
+
+/* ---- inspection of the last lookup (the reference's public Model members,
+ *      include/model.h:61-113); host output buffers, *n receives the count.
+ *      A NULL buffer or too small a capacity only reports *n. ---- */
+
+/* votes / voteCounts after the threshold, ordered by count descending then
+ * code ascending (src/cuda/model.cu:155-170); code = s_r<<32 | m_r<<6 | alpha. */
+ppf_status ppf_model_get_votes(ppf_model_t m, uint64_t* codes, uint32_t* counts, uint64_t cap,
+                               uint64_t* n);
+/* transformations (src/cuda/model.cu:191-200), U x 16 row-major. */
+ppf_status ppf_model_get_transformations(ppf_model_t m, float* T, uint64_t cap, uint64_t* n);
+/* transformation_trans (after clustering), transformation_rots, vote_counts_out
+ * (src/cuda/model.cu:202-244): U x 3, U x 4 (w,x,y,z), U. */
+ppf_status ppf_model_get_cluster_state(ppf_model_t m, float* trans, float* quats, float* scores,
+                                       uint64_t cap, uint64_t* n);
+/* ParallelHashArray of the model (include/impl/parallel_hash_array.hpp:16-47):
+ * unique keys, counts, first offsets (K each) and the key-sorted pair index
+ * map (P = n*n entries; pair = row*n + col). */
+ppf_status ppf_model_get_hash_array(ppf_model_t m, uint32_t* keys, uint32_t* counts,
+                                    uint32_t* first, uint64_t cap_k, uint32_t* map, uint64_t cap_p,
+                                    uint64_t* K, uint64_t* P);
+
+/* Keys of all n*n ordered pairs of a cloud, as Scene::initPPFs +
+ * ppf_hash_kernel produce them (src/cuda/scene.cu:64-99,
+ * src/cuda/kernel.cu:404-477): rows with index % ref_point_df != 0 and self
+ * pairs give 0.  keys is host or device memory of n*n uint32. */
+ppf_status ppf_pair_keys(ppf_context_t ctx, const float* xyz, const float* nxyz, uint64_t n,
+                         float d_dist, uint32_t ref_point_df, uint32_t* keys);
+
+/* Every nonzero (s_r, m_r, alpha) vote cell of a lookup in code order with its
+ * count: the reference's unique votes before the threshold
+ * (src/cuda/model.cu:148-151).  Runs the vote pass with no threshold; meant
+ * for small inputs. */
+ppf_status ppf_model_all_votes(ppf_model_t m, ppf_scene_t s, uint64_t* codes, uint32_t* counts,
+                               uint64_t cap, uint64_t* n);
+
+/* Per-scene-pair vote counts of ppf_vote_count_kernel
+ * (src/cuda/kernel.cu:480-501): counts[r*n_s + i] = model run length when
+ * scene pair (r, i) matches, else 0.  counts: host or device, n_s*n_s uint64. */
+ppf_status ppf_model_pair_vote_counts(ppf_model_t m, ppf_scene_t s, uint64_t* counts);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PPF_B200_H */

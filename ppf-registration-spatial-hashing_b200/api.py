@@ -1,0 +1,316 @@
+"""Python face of the engine, mirroring the reference's C++ API.
+
+``Model``, ``Scene`` and ``ppf_registration`` keep the reference's names,
+argument order and meaning (include/model.h:17-35, include/scene.h:15-16,
+include/ppf.h:9-15); results come back as numpy arrays.  Every call goes
+through libppf_b200.so; there is no CPU fallback.
+
+A cloud is anything with ``points`` and ``normals`` attributes, or a
+``(points, normals)`` pair, each ``(n, 3)`` float32: numpy arrays (host) or
+contiguous CUDA tensors (device, passed by pointer).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _capi
+
+
+class PPFError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{_capi.STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def _lib():
+    return _capi.load()
+
+
+def _check(status: int):
+    if status != _capi.PPF_OK:
+        msg = _lib().ppf_last_error()
+        raise PPFError(status, msg.decode() if msg else "")
+
+
+def _split_cloud(cloud):
+    if isinstance(cloud, (tuple, list)) and len(cloud) == 2:
+        return cloud[0], cloud[1]
+    return cloud.points, cloud.normals
+
+
+class _Buf:
+    """Pointer + length of a (n, 3) float32 array, host or device."""
+
+    def __init__(self, a, name):
+        if hasattr(a, "data_ptr") and hasattr(a, "is_cuda"):
+            if a.dtype.__repr__() != "torch.float32" or not a.is_contiguous() or a.dim() != 2 or a.shape[1] != 3:
+                raise ValueError(f"{name}: expected a contiguous (n, 3) float32 tensor")
+            self.keep = a
+            self.ptr = C.c_void_p(a.data_ptr())
+            self.n = int(a.shape[0])
+        else:
+            arr = np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+            if arr.ndim != 2 or arr.shape[1] != 3:
+                raise ValueError(f"{name}: expected an (n, 3) array")
+            self.keep = arr
+            self.ptr = C.c_void_p(arr.ctypes.data)
+            self.n = int(arr.shape[0])
+
+
+class Context:
+    """A device, a stream and a workspace (device index as devUse, src/cuda/ppf.cu:37-49)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        _check(_lib().ppf_context_create(int(device), C.byref(h)))
+        self.handle = h
+
+    def synchronize(self):
+        _check(_lib().ppf_context_synchronize(self.handle))
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(_lib().ppf_context_kernel_launches(self.handle))
+
+    @property
+    def stream(self) -> int:
+        return int(_lib().ppf_context_stream(self.handle) or 0)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _lib().ppf_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+class Scene:
+    """Scene(cloud, d_dist, ref_point_downsample_factor=1) (include/scene.h:15-16)."""
+
+    def __init__(self, cloud, d_dist: float, ref_point_downsample_factor: int = 1, context=None):
+        self.ctx = context or default_context()
+        p, q = _split_cloud(cloud)
+        bp, bq = _Buf(p, "points"), _Buf(q, "normals")
+        if bp.n != bq.n:
+            raise ValueError("points and normals differ in length")
+        h = C.c_void_p()
+        _check(
+            _lib().ppf_scene_create(
+                self.ctx.handle, bp.ptr, bq.ptr, bp.n, float(d_dist), int(ref_point_downsample_factor), C.byref(h)
+            )
+        )
+        self.handle = h
+        self.n = bp.n
+        self.d_dist = float(d_dist)
+        self.ref_point_downsample_factor = int(ref_point_downsample_factor)
+
+    def numPoints(self) -> int:
+        return self.n
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _lib().ppf_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Model:
+    """Model(cloud, d_dist, vote_count_threshold, cpu_clustering, use_l1_norm,
+    use_averaged_clusters) (include/model.h:17-19)."""
+
+    def __init__(self, cloud, d_dist: float, vote_count_threshold: float = 0.4, cpu_clustering: bool = False,
+                 use_l1_norm: bool = False, use_averaged_clusters: bool = False, context=None):
+        self.ctx = context or default_context()
+        p, q = _split_cloud(cloud)
+        bp, bq = _Buf(p, "points"), _Buf(q, "normals")
+        if bp.n != bq.n:
+            raise ValueError("points and normals differ in length")
+        h = C.c_void_p()
+        _check(
+            _lib().ppf_model_create(
+                self.ctx.handle, bp.ptr, bq.ptr, bp.n, float(d_dist), float(vote_count_threshold),
+                int(bool(cpu_clustering)), int(bool(use_l1_norm)), int(bool(use_averaged_clusters)), C.byref(h),
+            )
+        )
+        self.handle = h
+        self.n = bp.n
+        self.d_dist = float(d_dist)
+        self.vote_count_threshold = float(vote_count_threshold)
+        self.cpu_clustering = bool(cpu_clustering)
+        self.use_l1_norm = bool(use_l1_norm)
+        self.use_averaged_clusters = bool(use_averaged_clusters)
+        self.stats = None
+        self.pose = None
+
+    # Model::SetModelPointVoteWeights (src/cuda/model.cu:91-93)
+    def SetModelPointVoteWeights(self, weights):
+        w = np.ascontiguousarray(np.asarray(weights, dtype=np.float32))
+        _check(_lib().ppf_model_set_point_vote_weights(self.handle, C.c_void_p(w.ctypes.data), w.size))
+
+    # Model::ppf_lookup (src/cuda/model.cu:269-306) + pose extraction (src/cuda/ppf.cu:74-93)
+    def ppf_lookup(self, scene: Scene, raise_on_no_votes: bool = True) -> np.ndarray:
+        pose = np.zeros(16, np.float32)
+        st = _capi.ppf_stats()
+        status = _lib().ppf_model_lookup(self.handle, scene.handle, C.c_void_p(pose.ctypes.data), C.byref(st))
+        self.stats = st.as_dict()
+        self.pose = pose.reshape(4, 4)
+        if status == 4 and not raise_on_no_votes:
+            return self.pose
+        _check(status)
+        return self.pose
+
+    @property
+    def max_idx(self) -> int:
+        return int(self.stats["max_idx"]) if self.stats else 0
+
+    def _count(self, fn, *args):
+        n = C.c_uint64()
+        _check(fn(self.handle, *args, 0, C.byref(n)))
+        return int(n.value)
+
+    def get_votes(self):
+        """(codes uint64, counts uint32) of the kept votes in the reference's order."""
+        L = _lib()
+        n = self._count(L.ppf_model_get_votes, None, None)
+        codes = np.zeros(n, np.uint64)
+        counts = np.zeros(n, np.uint32)
+        m = C.c_uint64()
+        _check(L.ppf_model_get_votes(self.handle, codes.ctypes.data_as(_capi._u64p),
+                                     counts.ctypes.data_as(_capi._u32p), n, C.byref(m)))
+        return codes, counts
+
+    @property
+    def votes(self):
+        return self.get_votes()[0]
+
+    @property
+    def voteCounts(self):
+        return self.get_votes()[1]
+
+    def getTransformations(self) -> np.ndarray:
+        L = _lib()
+        n = self._count(L.ppf_model_get_transformations, None)
+        T = np.zeros((n, 16), np.float32)
+        m = C.c_uint64()
+        _check(L.ppf_model_get_transformations(self.handle, T.ctypes.data_as(_capi._fp), n, C.byref(m)))
+        return T
+
+    def get_cluster_state(self):
+        """(transformation_trans (U,3), transformation_rots (U,4), vote_counts_out (U,))."""
+        L = _lib()
+        n = self._count(L.ppf_model_get_cluster_state, None, None, None)
+        t = np.zeros((n, 3), np.float32)
+        q = np.zeros((n, 4), np.float32)
+        s = np.zeros(n, np.float32)
+        m = C.c_uint64()
+        _check(L.ppf_model_get_cluster_state(self.handle, t.ctypes.data_as(_capi._fp), q.ctypes.data_as(_capi._fp),
+                                             s.ctypes.data_as(_capi._fp), n, C.byref(m)))
+        return t, q, s
+
+    def hash_array(self):
+        """The model's ParallelHashArray: dict(keys, counts, first, map)."""
+        L = _lib()
+        K, P = C.c_uint64(), C.c_uint64()
+        _check(L.ppf_model_get_hash_array(self.handle, None, None, None, 0, None, 0, C.byref(K), C.byref(P)))
+        k = np.zeros(K.value, np.uint32)
+        c = np.zeros(K.value, np.uint32)
+        f = np.zeros(K.value, np.uint32)
+        mp = np.zeros(P.value, np.uint32)
+        _check(L.ppf_model_get_hash_array(
+            self.handle, k.ctypes.data_as(_capi._u32p), c.ctypes.data_as(_capi._u32p), f.ctypes.data_as(_capi._u32p),
+            K.value, mp.ctypes.data_as(_capi._u32p), P.value, C.byref(K), C.byref(P)))
+        return {"keys": k, "counts": c, "first": f, "map": mp}
+
+    def all_votes(self, scene: Scene):
+        """Every nonzero vote cell (code asc) with its count, before the threshold."""
+        L = _lib()
+        n = C.c_uint64()
+        _check(L.ppf_model_all_votes(self.handle, scene.handle, None, None, 0, C.byref(n)))
+        codes = np.zeros(n.value, np.uint64)
+        counts = np.zeros(n.value, np.uint32)
+        _check(L.ppf_model_all_votes(self.handle, scene.handle, codes.ctypes.data_as(_capi._u64p),
+                                     counts.ctypes.data_as(_capi._u32p), n.value, C.byref(n)))
+        return codes, counts
+
+    def pair_vote_counts(self, scene: Scene) -> np.ndarray:
+        out = np.zeros(scene.n * scene.n, np.uint64)
+        _check(_lib().ppf_model_pair_vote_counts(self.handle, scene.handle, C.c_void_p(out.ctypes.data)))
+        return out.reshape(scene.n, scene.n)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _lib().ppf_model_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def pair_keys(cloud, d_dist: float, ref_point_downsample_factor: int = 1, context=None) -> np.ndarray:
+    """Keys of all ordered pairs, (n, n) uint32 (Scene::initPPFs + ppf_hash_kernel)."""
+    ctx = context or default_context()
+    p, q = _split_cloud(cloud)
+    bp, bq = _Buf(p, "points"), _Buf(q, "normals")
+    out = np.zeros(bp.n * bp.n, np.uint32)
+    _check(_lib().ppf_pair_keys(ctx.handle, bp.ptr, bq.ptr, bp.n, float(d_dist), int(ref_point_downsample_factor),
+                                C.c_void_p(out.ctypes.data)))
+    return out.reshape(bp.n, bp.n)
+
+
+def ppf_registration(scene_clouds, model_clouds, model_d_dists, ref_point_downsample_factor=1,
+                     vote_count_threshold=0.4, cpu_clustering=False, use_l1_norm=False,
+                     use_averaged_clusters=False, devUse=0, model_weights=None, context=None,
+                     return_stats=False):
+    """ppf_registration (include/ppf.h:9-15): poses[i][j] of model j in scene i (4x4 float32)."""
+    L = _lib()
+    scenes = [tuple(_Buf(a, "scene") for a in _split_cloud(c)) for c in scene_clouds]
+    models = [tuple(_Buf(a, "model") for a in _split_cloud(c)) for c in model_clouds]
+    ns, nm = len(scenes), len(models)
+    sx = (C.c_void_p * max(ns, 1))(*[s[0].ptr for s in scenes])
+    sn = (C.c_void_p * max(ns, 1))(*[s[1].ptr for s in scenes])
+    sc = (C.c_uint64 * max(ns, 1))(*[s[0].n for s in scenes])
+    mx = (C.c_void_p * max(nm, 1))(*[m[0].ptr for m in models])
+    mn = (C.c_void_p * max(nm, 1))(*[m[1].ptr for m in models])
+    mc = (C.c_uint64 * max(nm, 1))(*[m[0].n for m in models])
+    dd = np.ascontiguousarray(np.asarray(model_d_dists, np.float32))
+    if dd.size != nm:
+        raise ValueError("one d_dist per model is required")
+    poses = np.zeros((max(ns, 1), max(nm, 1), 16), np.float32)
+    stats = (_capi.ppf_stats * max(ns * nm, 1))()
+    ctx_h = context.handle if context is not None else None
+    status = L.ppf_registration(
+        ctx_h, ns, sx, sn, sc, nm, mx, mn, mc, dd.ctypes.data_as(_capi._fp),
+        int(ref_point_downsample_factor), float(vote_count_threshold), int(bool(cpu_clustering)),
+        int(bool(use_l1_norm)), int(bool(use_averaged_clusters)), int(devUse), None,
+        C.c_void_p(poses.ctypes.data), stats,
+    )
+    if status not in (0, 4):
+        _check(status)
+    out = [[poses[i, j].reshape(4, 4).copy() for j in range(nm)] for i in range(ns)]
+    if return_stats:
+        return out, [[stats[i * nm + j].as_dict() for j in range(nm)] for i in range(ns)]
+    return out

@@ -1,0 +1,462 @@
+// Host orchestration and the C ABI (include/ppf_b200.h).  Every entry point
+// catches engine errors and returns a status; the message is kept per thread.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+
+namespace ppf {
+
+Context::~Context() {
+  for (auto& e : ev)
+    if (e) cudaEventDestroy(e);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+namespace {
+
+thread_local std::string g_last_error;
+
+ppf_status fail(ppf_status s, const std::string& msg) {
+  g_last_error = msg;
+  return s;
+}
+
+template <typename F>
+ppf_status guarded(F&& f) {
+  try {
+    g_last_error.clear();
+    return f();
+  } catch (const Error& e) {
+    return fail(e.status, e.what());
+  } catch (const std::bad_alloc&) {
+    return fail(PPF_ERR_OUT_OF_MEMORY, "host allocation failed");
+  } catch (const std::exception& e) {
+    return fail(PPF_ERR_INTERNAL, e.what());
+  }
+}
+
+void copy_out(void* dst, const void* src_dev, size_t bytes, cudaStream_t st) {
+  if (!dst || !bytes) return;
+  PPF_CUDA(cudaMemcpyAsync(dst, src_dev, bytes, cudaMemcpyDefault, st));
+}
+
+constexpr size_t kInitialCandidates = size_t(1) << 22;
+
+struct LookupOut {
+  ppf_status status = PPF_OK;
+  float pose[16] = {0};
+  ppf_stats stats{};
+};
+
+// Model::ppf_lookup + the pose extraction of ppf_registration.
+LookupOut lookup(Model& m, const SceneData& s) {
+  Context& ctx = *m.ctx;
+  LookupState& st = m.last;
+  LookupOut out;
+  const size_t launches0 = ctx.launches;
+  PPF_CUDA(cudaEventRecord(ctx.ev[2], ctx.stream));
+  size_t cap = std::max(kInitialCandidates, st.cand_codes.bytes / sizeof(unsigned long long));
+  VoteResult vr = run_votes(ctx, m, s, st, false, -1.f, cap);
+  st.U = 0;
+  out.stats.n_votes = vr.n_votes;
+  out.stats.n_matched_pairs = vr.n_matched;
+  out.stats.n_exact_bins = vr.n_exact;
+  out.stats.max_vote_count = vr.max_count;
+  out.stats.vote_ms = vr.vote_ms;
+  if (vr.max_count == 0) {
+    out.status = PPF_ERR_NO_VOTES;
+    return out;
+  }
+  const float min_votecount = m.vote_count_threshold * (float)vr.max_count;
+  out.stats.min_votecount = min_votecount;
+  if (vr.n_cand > cap) {
+    // Emission buffer overflowed: run again with the final threshold, which
+    // emits exactly the kept cells (at most n_cand of them).
+    cap = vr.n_cand;
+    VoteResult vr2 = run_votes(ctx, m, s, st, false, min_votecount, cap);
+    PPF_REQUIRE(vr2.n_cand <= cap && vr2.max_count == vr.max_count, PPF_ERR_INTERNAL,
+                "vote pass is not reproducible");
+    out.stats.vote_ms += vr2.vote_ms;
+    vr.n_cand = vr2.n_cand;
+  }
+  out.stats.n_candidates = vr.n_cand;
+  const size_t U = select_votes(ctx, m, s, st, vr.n_cand, min_votecount);
+  out.stats.n_kept = U;
+  if (U == 0) {
+    out.status = PPF_ERR_NO_VOTES;
+    return out;
+  }
+  compute_poses(ctx, m, s, st);
+  if (m.cpu_clustering) {
+    std::vector<float> T(U * 16);
+    std::vector<uint32_t> cnt(U);
+    PPF_CUDA(cudaMemcpyAsync(T.data(), st.transforms.ptr, U * 64, cudaMemcpyDeviceToHost, ctx.stream));
+    PPF_CUDA(cudaMemcpyAsync(cnt.data(), st.counts.ptr, U * 4, cudaMemcpyDeviceToHost, ctx.stream));
+    PPF_CUDA(cudaStreamSynchronize(ctx.stream));
+    float poses[48];
+    uint32_t votes[3];
+    int nc = cluster_poses_cpu(T.data(), cnt.data(), U, m.t.d_dist, PPF_D_ANGLE_HOST, poses, votes);
+    st.cpu_poses.assign(poses, poses + 16 * nc);
+    if (nc > 0) std::memcpy(out.pose, poses, sizeof(out.pose));
+    out.stats.max_idx = 0;
+    out.stats.best_score = nc > 0 ? (float)votes[0] : 0.f;
+  } else {
+    float best_score = 0;
+    size_t idx = cluster_poses_gpu(ctx, m, st, &best_score);
+    PPF_CUDA(cudaMemcpyAsync(out.pose, st.best.ptr, sizeof(out.pose), cudaMemcpyDeviceToHost, ctx.stream));
+    out.stats.max_idx = idx;
+    out.stats.best_score = best_score;
+  }
+  PPF_CUDA(cudaEventRecord(ctx.ev[3], ctx.stream));
+  PPF_CUDA(cudaStreamSynchronize(ctx.stream));
+  uint32_t flags = 0;
+  PPF_CUDA(cudaMemcpy(&flags, ctx.flags.ptr, 4, cudaMemcpyDeviceToHost));
+  PPF_REQUIRE(!(flags & kFlagSpinTimeout), PPF_ERR_TIMEOUT, "radix sort look-back timed out");
+  PPF_CUDA(cudaEventElapsedTime(&out.stats.total_ms, ctx.ev[2], ctx.ev[3]));
+  out.stats.gpu_launches = (uint32_t)(ctx.launches - launches0);
+  return out;
+}
+
+void check_cloud(const float* xyz, const float* nxyz, uint64_t n) {
+  PPF_REQUIRE(xyz && nxyz, PPF_ERR_INVALID_ARGUMENT, "null point or normal pointer");
+  PPF_REQUIRE(n >= 1, PPF_ERR_INVALID_ARGUMENT, "empty cloud");
+}
+
+void init_context(Context& c, int device) {
+  int count = 0;
+  PPF_CUDA(cudaGetDeviceCount(&count));
+  PPF_REQUIRE(count > 0, PPF_ERR_CUDA, "no CUDA device");
+  c.device = std::max(0, std::min(count - 1, device));
+  PPF_CUDA(cudaSetDevice(c.device));
+  PPF_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+  for (auto& e : c.ev) PPF_CUDA(cudaEventCreate(&e));
+  c.flags.reserve(256);
+  c.counters.reserve(256);
+  PPF_CUDA(cudaMemset(c.flags.ptr, 0, 256));
+  int optin = 0;
+  PPF_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device));
+  c.vote_smem_limit = optin - 2048;  // static shared memory of the vote kernel
+}
+
+}  // namespace
+}  // namespace ppf
+
+using namespace ppf;
+
+extern "C" {
+
+const char* ppf_last_error(void) { return g_last_error.c_str(); }
+int ppf_abi_version(void) { return PPF_B200_ABI_VERSION; }
+
+ppf_status ppf_context_create(int device, ppf_context_t* out) {
+  return guarded([&]() {
+    PPF_REQUIRE(out, PPF_ERR_INVALID_ARGUMENT, "null output handle");
+    std::unique_ptr<ppf_context_s> c(new ppf_context_s());
+    init_context(c->c, device);
+    *out = c.release();
+    return PPF_OK;
+  });
+}
+
+ppf_status ppf_context_destroy(ppf_context_t ctx) {
+  return guarded([&]() {
+    if (ctx) {
+      cudaSetDevice(ctx->c.device);
+      cudaStreamSynchronize(ctx->c.stream);
+      delete ctx;
+    }
+    return PPF_OK;
+  });
+}
+
+ppf_status ppf_context_synchronize(ppf_context_t ctx) {
+  return guarded([&]() {
+    PPF_REQUIRE(ctx, PPF_ERR_INVALID_ARGUMENT, "null context");
+    PPF_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    return PPF_OK;
+  });
+}
+
+void* ppf_context_stream(ppf_context_t ctx) { return ctx ? (void*)ctx->c.stream : nullptr; }
+uint64_t ppf_context_kernel_launches(ppf_context_t ctx) { return ctx ? ctx->c.launches : 0; }
+
+ppf_status ppf_model_create(ppf_context_t ctx, const float* xyz, const float* nxyz, uint64_t n,
+                            float d_dist, float vote_count_threshold, int cpu_clustering,
+                            int use_l1_norm, int use_averaged_clusters, ppf_model_t* out) {
+  return guarded([&]() {
+    PPF_REQUIRE(ctx && out, PPF_ERR_INVALID_ARGUMENT, "null context or output handle");
+    check_cloud(xyz, nxyz, n);
+    PPF_REQUIRE(std::isfinite(vote_count_threshold) && vote_count_threshold >= 0.f,
+                PPF_ERR_INVALID_ARGUMENT, "vote_count_threshold must be finite and >= 0");
+    PPF_CUDA(cudaSetDevice(ctx->c.device));
+    std::unique_ptr<ppf_model_s> m(new ppf_model_s());
+    m->m.ctx = &ctx->c;
+    m->m.vote_count_threshold = vote_count_threshold;
+    m->m.cpu_clustering = cpu_clustering != 0;
+    m->m.use_l1_norm = use_l1_norm != 0;
+    m->m.use_averaged_clusters = use_averaged_clusters != 0;
+    build_model(ctx->c, m->m.t, xyz, nxyz, n, d_dist);
+    *out = m.release();
+    return PPF_OK;
+  });
+}
+
+ppf_status ppf_model_set_point_vote_weights(ppf_model_t m, const float* w, uint64_t n) {
+  return guarded([&]() {
+    PPF_REQUIRE(m && w, PPF_ERR_INVALID_ARGUMENT, "null model or weights");
+    PPF_REQUIRE(n == m->m.t.n, PPF_ERR_INVALID_ARGUMENT, "one weight per model point required");
+    PPF_CUDA(cudaSetDevice(m->m.ctx->device));
+    PPF_CUDA(cudaMemcpyAsync(m->m.t.weights.ptr, w, n * sizeof(float), cudaMemcpyDefault,
+                             m->m.ctx->stream));
+    PPF_CUDA(cudaStreamSynchronize(m->m.ctx->stream));
+    return PPF_OK;
+  });
+}
+
+ppf_status ppf_model_destroy(ppf_model_t m) {
+  return guarded([&]() {
+    if (m) {
+      cudaSetDevice(m->m.ctx->device);
+      cudaStreamSynchronize(m->m.ctx->stream);
+      delete m;
+    }
+    return PPF_OK;
+  });
+}
+
+uint64_t ppf_model_num_points(ppf_model_t m) { return m ? m->m.t.n : 0; }
+uint64_t ppf_model_num_keys(ppf_model_t m) { return m ? m->m.t.K : 0; }
+
+ppf_status ppf_scene_create(ppf_context_t ctx, const float* xyz, const float* nxyz, uint64_t n,
+                            float d_dist, uint32_t ref_point_df, ppf_scene_t* out) {
+  return guarded([&]() {
+    PPF_REQUIRE(ctx && out, PPF_ERR_INVALID_ARGUMENT, "null context or output handle");
+    check_cloud(xyz, nxyz, n);
+    PPF_REQUIRE(n < (1ull << 31), PPF_ERR_INVALID_ARGUMENT, "scene larger than 2^31 points");
+    PPF_REQUIRE(d_dist > 0.f && std::isfinite(d_dist), PPF_ERR_INVALID_ARGUMENT,
+                "d_dist must be a positive finite number");
+    PPF_CUDA(cudaSetDevice(ctx->c.device));
+    std::unique_ptr<ppf_scene_s> s(new ppf_scene_s());
+    s->ctx = &ctx->c;
+    s->s.n = (uint32_t)n;
+    s->s.d_dist = d_dist;
+    s->s.ref_df = ref_point_df ? ref_point_df : 1;
+    upload_points(ctx->c, xyz, n, s->s.pts);
+    upload_points(ctx->c, nxyz, n, s->s.nrm);
+    *out = s.release();
+    return PPF_OK;
+  });
+}
+
+ppf_status ppf_scene_destroy(ppf_scene_t s) {
+  return guarded([&]() {
+    if (s) {
+      cudaSetDevice(s->ctx->device);
+      cudaStreamSynchronize(s->ctx->stream);
+      delete s;
+    }
+    return PPF_OK;
+  });
+}
+
+ppf_status ppf_model_lookup(ppf_model_t m, ppf_scene_t s, float* pose_out, ppf_stats* stats) {
+  return guarded([&]() {
+    PPF_REQUIRE(m && s && pose_out, PPF_ERR_INVALID_ARGUMENT, "null model, scene or pose");
+    PPF_REQUIRE(m->m.ctx == s->ctx, PPF_ERR_INVALID_ARGUMENT, "model and scene on different contexts");
+    PPF_CUDA(cudaSetDevice(m->m.ctx->device));
+    LookupOut r = lookup(m->m, s->s);
+    PPF_CUDA(cudaMemcpy(pose_out, r.pose, sizeof(r.pose), cudaMemcpyDefault));
+    if (stats) *stats = r.stats;
+    if (r.status != PPF_OK) return fail(r.status, "no vote passed the threshold");
+    return PPF_OK;
+  });
+}
+
+ppf_status ppf_registration(ppf_context_t ctx, uint64_t n_scenes, const float* const* scene_xyz,
+                            const float* const* scene_nxyz, const uint64_t* scene_n,
+                            uint64_t n_models, const float* const* model_xyz,
+                            const float* const* model_nxyz, const uint64_t* model_n,
+                            const float* model_d_dists, uint32_t ref_point_df,
+                            float vote_count_threshold, int cpu_clustering, int use_l1_norm,
+                            int use_averaged_clusters, int dev_use, const float* model_weights,
+                            float* poses_out, ppf_stats* stats_out) {
+  (void)model_weights;  // accepted and unused, as src/cuda/ppf.cu:35
+  return guarded([&]() {
+    PPF_REQUIRE(poses_out || (n_scenes * n_models == 0), PPF_ERR_INVALID_ARGUMENT, "null pose output");
+    PPF_REQUIRE(n_models == 0 || (model_xyz && model_nxyz && model_n && model_d_dists),
+                PPF_ERR_INVALID_ARGUMENT, "null model arrays");
+    PPF_REQUIRE(n_scenes == 0 || (scene_xyz && scene_nxyz && scene_n), PPF_ERR_INVALID_ARGUMENT,
+                "null scene arrays");
+    std::unique_ptr<ppf_context_s> own;
+    ppf_context_t c = ctx;
+    if (!c) {
+      own.reset(new ppf_context_s());
+      init_context(own->c, dev_use);
+      c = own.get();
+    }
+    PPF_CUDA(cudaSetDevice(c->c.device));
+    std::vector<float> host_poses(n_scenes * n_models * 16, 0.f);
+    ppf_status worst = PPF_OK;
+    for (uint64_t j = 0; j < n_models; ++j) {
+      ppf_model_t m = nullptr;
+      ppf_status st = ppf_model_create(c, model_xyz[j], model_nxyz[j], model_n[j], model_d_dists[j],
+                                       vote_count_threshold, cpu_clustering, use_l1_norm,
+                                       use_averaged_clusters, &m);
+      if (st != PPF_OK) throw Error(st, g_last_error);
+      std::unique_ptr<ppf_model_s, ppf_status (*)(ppf_model_t)> mg(m, ppf_model_destroy);
+      for (uint64_t i = 0; i < n_scenes; ++i) {
+        ppf_scene_t s = nullptr;
+        st = ppf_scene_create(c, scene_xyz[i], scene_nxyz[i], scene_n[i], model_d_dists[j],
+                              ref_point_df, &s);
+        if (st != PPF_OK) throw Error(st, g_last_error);
+        std::unique_ptr<ppf_scene_s, ppf_status (*)(ppf_scene_t)> sg(s, ppf_scene_destroy);
+        LookupOut r = lookup(m->m, s->s);
+        std::memcpy(&host_poses[(i * n_models + j) * 16], r.pose, sizeof(r.pose));
+        if (stats_out) stats_out[i * n_models + j] = r.stats;
+        if (r.status != PPF_OK) worst = r.status;
+      }
+    }
+    if (!host_poses.empty())
+      PPF_CUDA(cudaMemcpy(poses_out, host_poses.data(), host_poses.size() * sizeof(float),
+                          cudaMemcpyDefault));
+    if (worst != PPF_OK) return fail(worst, "at least one (scene, model) pair had no votes");
+    return PPF_OK;
+  });
+}
+
+ppf_status ppf_model_get_votes(ppf_model_t m, uint64_t* codes, uint32_t* counts, uint64_t cap,
+                               uint64_t* n) {
+  return guarded([&]() {
+    PPF_REQUIRE(m && n, PPF_ERR_INVALID_ARGUMENT, "null model or count");
+    const size_t U = m->m.last.U;
+    *n = U;
+    if (U && cap >= U) {
+      copy_out(codes, m->m.last.codes.ptr, U * 8, m->m.ctx->stream);
+      copy_out(counts, m->m.last.counts.ptr, U * 4, m->m.ctx->stream);
+      PPF_CUDA(cudaStreamSynchronize(m->m.ctx->stream));
+    }
+    return PPF_OK;
+  });
+}
+
+ppf_status ppf_model_get_transformations(ppf_model_t m, float* T, uint64_t cap, uint64_t* n) {
+  return guarded([&]() {
+    PPF_REQUIRE(m && n, PPF_ERR_INVALID_ARGUMENT, "null model or count");
+    const size_t U = m->m.last.U;
+    *n = U;
+    if (U && cap >= U) {
+      copy_out(T, m->m.last.transforms.ptr, U * 64, m->m.ctx->stream);
+      PPF_CUDA(cudaStreamSynchronize(m->m.ctx->stream));
+    }
+    return PPF_OK;
+  });
+}
+
+ppf_status ppf_model_get_cluster_state(ppf_model_t m, float* trans, float* quats, float* scores,
+                                       uint64_t cap, uint64_t* n) {
+  return guarded([&]() {
+    PPF_REQUIRE(m && n, PPF_ERR_INVALID_ARGUMENT, "null model or count");
+    const size_t U = m->m.last.U;
+    *n = U;
+    if (U && cap >= U && !m->m.cpu_clustering) {
+      copy_out(trans, m->m.last.trans.ptr, U * 12, m->m.ctx->stream);
+      copy_out(quats, m->m.last.quats.ptr, U * 16, m->m.ctx->stream);
+      copy_out(scores, m->m.last.scores.ptr, U * 4, m->m.ctx->stream);
+      PPF_CUDA(cudaStreamSynchronize(m->m.ctx->stream));
+    }
+    return PPF_OK;
+  });
+}
+
+ppf_status ppf_model_get_hash_array(ppf_model_t m, uint32_t* keys, uint32_t* counts,
+                                    uint32_t* first, uint64_t cap_k, uint32_t* map, uint64_t cap_p,
+                                    uint64_t* K, uint64_t* P) {
+  return guarded([&]() {
+    PPF_REQUIRE(m && K && P, PPF_ERR_INVALID_ARGUMENT, "null model or sizes");
+    const ModelTables& t = m->m.t;
+    *K = t.K;
+    *P = t.P;
+    cudaStream_t st = m->m.ctx->stream;
+    if (cap_k >= t.K) {
+      copy_out(keys, t.uniq.ptr, t.K * 4, st);
+      copy_out(counts, t.count.ptr, t.K * 4, st);
+      copy_out(first, t.first.ptr, t.K * 4, st);
+    }
+    if (cap_p >= t.P) copy_out(map, t.pairs.ptr, t.P * 4, st);
+    PPF_CUDA(cudaStreamSynchronize(st));
+    return PPF_OK;
+  });
+}
+
+ppf_status ppf_pair_keys(ppf_context_t ctx, const float* xyz, const float* nxyz, uint64_t n,
+                         float d_dist, uint32_t ref_point_df, uint32_t* keys) {
+  return guarded([&]() {
+    PPF_REQUIRE(ctx && keys, PPF_ERR_INVALID_ARGUMENT, "null context or keys");
+    check_cloud(xyz, nxyz, n);
+    PPF_REQUIRE(n <= 65535, PPF_ERR_INVALID_ARGUMENT, "pair keys limited to 65535 points");
+    Context& c = ctx->c;
+    PPF_CUDA(cudaSetDevice(c.device));
+    DevBuf p, q, k;
+    upload_points(c, xyz, n, p);
+    upload_points(c, nxyz, n, q);
+    uint32_t* dst = keys;
+    if (!is_device_pointer(keys)) {
+      k.reserve(n * n * 4);
+      dst = k.as<uint32_t>();
+    }
+    pair_keys_device(c, p.as<float4>(), q.as<float4>(), (uint32_t)n, ref_point_df, d_dist, dst);
+    if (dst != keys) PPF_CUDA(cudaMemcpyAsync(keys, dst, n * n * 4, cudaMemcpyDeviceToHost, c.stream));
+    PPF_CUDA(cudaStreamSynchronize(c.stream));
+    return PPF_OK;
+  });
+}
+
+ppf_status ppf_model_all_votes(ppf_model_t m, ppf_scene_t s, uint64_t* codes, uint32_t* counts,
+                               uint64_t cap, uint64_t* n) {
+  return guarded([&]() {
+    PPF_REQUIRE(m && s && n, PPF_ERR_INVALID_ARGUMENT, "null model, scene or count");
+    Context& c = *m->m.ctx;
+    PPF_CUDA(cudaSetDevice(c.device));
+    LookupState& st = m->m.last;
+    size_t want = (size_t)((s->s.n + s->s.ref_df - 1) / s->s.ref_df) * m->m.t.n * kBins;
+    size_t capc = std::min<size_t>(std::max<size_t>(want, 1), size_t(1) << 28);
+    VoteResult vr = run_votes(c, m->m, s->s, st, true, -1.f, capc);
+    PPF_REQUIRE(vr.n_cand <= capc, PPF_ERR_OUT_OF_MEMORY, "too many vote cells for a dump");
+    sort_by_code(c, st, vr.n_cand);
+    st.U = 0;
+    *n = vr.n_cand;
+    if (cap >= vr.n_cand) {
+      copy_out(codes, st.codes.ptr, vr.n_cand * 8, c.stream);
+      copy_out(counts, st.counts.ptr, vr.n_cand * 4, c.stream);
+    }
+    PPF_CUDA(cudaStreamSynchronize(c.stream));
+    return PPF_OK;
+  });
+}
+
+ppf_status ppf_model_pair_vote_counts(ppf_model_t m, ppf_scene_t s, uint64_t* counts) {
+  return guarded([&]() {
+    PPF_REQUIRE(m && s && counts, PPF_ERR_INVALID_ARGUMENT, "null model, scene or counts");
+    Context& c = *m->m.ctx;
+    PPF_CUDA(cudaSetDevice(c.device));
+    const size_t nn = (size_t)s->s.n * s->s.n;
+    DevBuf tmp;
+    uint64_t* dst = counts;
+    if (!is_device_pointer(counts)) {
+      tmp.reserve(nn * 8);
+      dst = tmp.as<uint64_t>();
+    }
+    pair_vote_counts(c, m->m, s->s, dst);
+    if (dst != counts) PPF_CUDA(cudaMemcpyAsync(counts, dst, nn * 8, cudaMemcpyDeviceToHost, c.stream));
+    PPF_CUDA(cudaStreamSynchronize(c.stream));
+    return PPF_OK;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,148 @@
+// Engine objects behind the C ABI: context, resident model hash arrays,
+// resident scenes, and the device-side layout the kernels consume.
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+#include "sort_scan.cuh"
+
+struct ppf_context_s;
+
+namespace ppf {
+
+// Angle bins per model reference point in the vote accumulator (alpha bins
+// 0..30; bin 30 is only reached at alpha == pi exactly).
+constexpr int kBins = 31;
+// Vote kernel launch shape.
+constexpr int kVoteThreads = 512;
+constexpr int kVoteWarps = kVoteThreads / 32;
+// Angle quantum on the host (include/kernel.h:16 evaluated in float).
+#define PPF_D_ANGLE_HOST ((2.0f * 3.141592654f) / float(30))
+
+struct Context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  RadixSorter<uint32_t> sort32;
+  RadixSorter<unsigned long long> sort64;
+  DevBuf flags;      // uint32 device flags (kFlag*)
+  DevBuf counters;   // small device counters for kernels
+  DevBuf scratch;    // run-table scratch
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  int vote_smem_limit = 0;  // max dynamic shared memory per vote block
+  size_t launches = 0;      // kernels launched (running total)
+  ~Context();
+};
+
+// Model hash array resident in HBM (built once by ppf_model_create).
+struct ModelTables {
+  uint32_t n = 0;        // model points
+  float d_dist = 0;
+  // per model point
+  DevBuf pts, nrm;       // float4 (x, y, z, 0)
+  DevBuf frame_r1, frame_r2;  // rows 1 and 2 of the point's reference frame
+  DevBuf angles;         // float2 (roty, rotz) of the frame
+  DevBuf weights;        // float vote weights (default 1)
+  // all ordered pairs, sorted by feature key (stable: pair index order)
+  size_t P = 0;
+  DevBuf keys;           // uint32 sorted keys
+  DevBuf pairs;          // uint32 pair index r*n + i (the hash array's data map)
+  DevBuf entries;        // uint32 (m_r << 16) | 16-bit angle of u
+  // runs
+  size_t K = 0;
+  DevBuf uniq, first, count;  // uint32 each
+  DevBuf run_flags;           // uint8: 1 = run holds a degenerate pair (exact bins only)
+  // key -> run open-addressing table (key 0 is the empty marker)
+  DevBuf ht_keys, ht_runs;
+  uint32_t ht_mask = 0;
+  // m_r chunking of the vote accumulator
+  uint32_t chunk = 0, n_chunks = 0;
+  DevBuf split;  // uint32 [K * (n_chunks + 1)] first run position per chunk
+};
+
+struct SceneData {
+  uint32_t n = 0;
+  float d_dist = 0;
+  uint32_t ref_df = 1;
+  DevBuf pts, nrm;  // float4
+};
+
+// Results of the last lookup, kept on the device for the inspection calls.
+struct LookupState {
+  size_t U = 0;
+  DevBuf codes;       // uint64 kept vote codes, reference order
+  DevBuf counts;      // uint32
+  DevBuf weighted;    // float
+  DevBuf transforms;  // float U*16
+  DevBuf trans;       // float U*3 (after clustering)
+  DevBuf trans0;      // float U*3 (before clustering)
+  DevBuf quats;       // float U*4
+  DevBuf cell_keys;   // uint32 U
+  DevBuf adj;         // uint32 U*27
+  DevBuf scores;      // float U
+  DevBuf cells_sorted, cells_map, cells_uniq, cells_first, cells_count;
+  DevBuf cand_codes, cand_counts;  // vote-pass candidates
+  DevBuf tmp64, tmp32a, tmp32b, perm;
+  DevBuf best;        // float[16] pose + int idx
+  std::vector<float> cpu_poses;
+};
+
+struct Model {
+  Context* ctx = nullptr;
+  ModelTables t;
+  float vote_count_threshold = 0.4f;
+  bool cpu_clustering = false, use_l1_norm = false, use_averaged_clusters = false;
+  LookupState last;
+};
+
+// ---- model build (model.cu)
+void build_model(Context& ctx, ModelTables& t, const float* xyz, const float* nxyz, size_t n,
+                 float d_dist);
+// keys of all n*n ordered pairs of a cloud held as float4 device arrays
+void pair_keys_device(Context& ctx, const float4* pts, const float4* nrm, uint32_t n,
+                      uint32_t ref_df, float d_dist, uint32_t* keys);
+// upload n x 3 floats (host or device) into a float4 device array
+void upload_points(Context& ctx, const float* xyz, size_t n, DevBuf& dst);
+bool is_device_pointer(const void* p);
+
+// ---- voting (vote.cu)
+struct VoteResult {
+  uint32_t max_count = 0;
+  uint64_t n_votes = 0, n_matched = 0, n_exact = 0;
+  uint64_t n_cand = 0;
+  float vote_ms = 0;
+};
+// Runs the vote pass.  emit_all: emit every nonzero cell (no threshold).
+// floor >= 0 forces the emission floor (used when re-running after a
+// candidate-buffer overflow).  Candidates land in st.cand_codes/cand_counts.
+VoteResult run_votes(Context& ctx, const Model& m, const SceneData& s, LookupState& st,
+                     bool emit_all, float floor, size_t cand_cap);
+void pair_vote_counts(Context& ctx, const Model& m, const SceneData& s, uint64_t* out_dev);
+
+// ---- poses and clustering (pose.cu)
+// Filters the candidates to the kept votes and orders them (count desc,
+// code asc); returns U.
+size_t select_votes(Context& ctx, const Model& m, const SceneData& s, LookupState& st,
+                    size_t n_cand, float min_votecount);
+// Orders arbitrary (code, count) pairs by code ascending (all-votes dump).
+void sort_by_code(Context& ctx, LookupState& st, size_t n);
+void compute_poses(Context& ctx, const Model& m, const SceneData& s, LookupState& st);
+// GPU clustering + argmax; writes the best pose into st.best and returns the index.
+size_t cluster_poses_gpu(Context& ctx, const Model& m, LookupState& st, float* best_score);
+
+// ---- greedy CPU clustering (cpu_cluster.cpp)
+int cluster_poses_cpu(const float* poses, const uint32_t* votes, size_t n, float trans_thresh,
+                      float rot_thresh, float out_poses[3 * 16], uint32_t out_votes[3]);
+
+}  // namespace ppf
+
+struct ppf_context_s {
+  ppf::Context c;
+};
+struct ppf_model_s {
+  ppf::Model m;
+};
+struct ppf_scene_s {
+  ppf::Context* ctx = nullptr;
+  ppf::SceneData s;
+};

@@ -1,0 +1,381 @@
+// After the vote pass: threshold and order the votes, one pose per kept vote,
+// spatial-hash pose clustering and the best pose
+// (src/cuda/model.cu:155-244,293-295, src/cuda/ppf.cu:78-93).
+#include <algorithm>
+#include <cstring>
+
+#include "engine.h"
+#include "ppf_math.cuh"
+
+namespace ppf {
+namespace {
+
+// Keep candidates with count > min_votecount (compared in float, as the
+// reference's count_if lambda does, src/cuda/model.cu:164-167).
+__global__ void filter_kernel(const unsigned long long* __restrict__ code,
+                              const uint32_t* __restrict__ count, size_t n, float min_votecount,
+                              unsigned long long* __restrict__ out_code, uint32_t* __restrict__ out_count,
+                              uint32_t* __restrict__ n_out) {
+  const int lane = threadIdx.x & 31;
+  for (size_t b = blockIdx.x * (size_t)blockDim.x; b < n; b += (size_t)gridDim.x * blockDim.x) {
+    size_t i = b + threadIdx.x;
+    bool keep = i < n && (float)count[i] > min_votecount;
+    uint32_t ballot = __ballot_sync(0xffffffffu, keep);
+    if (!ballot) continue;
+    uint32_t s0 = 0;
+    if (lane == 0) s0 = atomicAdd(n_out, (uint32_t)__popc(ballot));
+    s0 = __shfl_sync(0xffffffffu, s0, 0);
+    if (keep) {
+      uint32_t s = s0 + __popc(ballot & ((1u << lane) - 1u));
+      out_code[s] = code[i];
+      out_count[s] = count[i];
+    }
+  }
+}
+
+// Descending order of the count as a float (the reference sorts with
+// thrust::greater<float>, src/cuda/model.cu:155-158): complement of the
+// float's bits, which are monotone for non-negative floats.
+__global__ void count_key_kernel(const uint32_t* __restrict__ count, size_t n,
+                                 uint32_t* __restrict__ key) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    key[i] = ~__float_as_uint((float)count[i]);
+}
+
+__global__ void gather_kernel(const uint32_t* __restrict__ perm,
+                              const unsigned long long* __restrict__ code_in,
+                              const uint32_t* __restrict__ count_in, size_t n,
+                              unsigned long long* __restrict__ code_out,
+                              uint32_t* __restrict__ count_out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    uint32_t p = perm[i];
+    code_out[i] = code_in[p];
+    count_out[i] = count_in[p];
+  }
+}
+
+struct PoseArgs {
+  const unsigned long long* codes;
+  const uint32_t* counts;
+  size_t U;
+  const float4* m_pts;
+  const float2* m_ang;
+  const float* m_w;
+  const float4* s_pts;
+  const float4* s_nrm;
+  float d_dist;
+  float* transforms;
+  float* trans0;
+  float* quats;
+  float* weighted;
+  uint32_t* cell_keys;
+  uint32_t* adj;
+};
+
+// trans_calc_kernel2 + vote_weight_kernel + mat2transquat_kernel +
+// trans2idx_kernel (src/cuda/kernel.cu:605-699,766-782) for one kept vote.
+__global__ void poses_kernel(PoseArgs a) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < a.U;
+       i += (size_t)gridDim.x * blockDim.x) {
+    unsigned long long code = a.codes[i];
+    uint32_t sr = (uint32_t)(code >> 32), mc = (uint32_t)code;
+    uint32_t mr = mc >> 6, bin = mc & 63u;
+    float T[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) T[k] = 0.f;
+    if (!(sr == 0 && mr == 0 && bin == 0)) {  // vote code 0 is skipped (kernel.cu:628)
+      float4 mp = a.m_pts[mr];
+      float2 ma2 = a.m_ang[mr];
+      FrameAngles ma;
+      ma.roty = ma2.x;
+      ma.rotz = ma2.y;
+      float4 sp = a.s_pts[sr], sn = a.s_nrm[sr];
+      FrameAngles sa = frame_angles(make_float3(sn.x, sn.y, sn.z));
+      vote_pose(bin, make_float3(mp.x, mp.y, mp.z), ma, make_float3(sp.x, sp.y, sp.z), sa, T);
+    }
+    float* Tout = a.transforms + 16 * i;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) Tout[k] = T[k];
+    float3 t = make_float3(T[3], T[7], T[11]);
+    a.trans0[3 * i] = t.x;
+    a.trans0[3 * i + 1] = t.y;
+    a.trans0[3 * i + 2] = t.z;
+    float4 q = pose_quaternion(T);
+    a.quats[4 * i] = q.x;
+    a.quats[4 * i + 1] = q.y;
+    a.quats[4 * i + 2] = q.z;
+    a.quats[4 * i + 3] = q.w;
+    a.weighted[i] = a.m_w[mr] * a.counts[i];
+    int3 c = trans_cell(t, a.d_dist);
+    a.cell_keys[i] = cell_key(c.x, c.y, c.z);
+    uint32_t* adj = a.adj + 27 * i;
+    int idx = 0;
+    for (int di = -1; di < 2; ++di)
+      for (int dj = -1; dj < 2; ++dj)
+        for (int dk = -1; dk < 2; ++dk, ++idx)
+          adj[idx] = (di == 0 && dj == 0 && dk == 0) ? 0u : cell_key(c.x + di, c.y + dj, c.z + dk);
+  }
+}
+
+struct ClusterArgs {
+  size_t U;
+  const float* trans0;
+  const float* quats;
+  const float* weighted;
+  const uint32_t* adj;
+  const uint32_t* uniq;
+  const uint32_t* first;
+  const uint32_t* count;
+  const uint32_t* map;
+  size_t Kc;
+  float d_dist;
+  int use_l1, use_avg;
+  float* scores;
+  float* trans;
+};
+
+// rot_clustering_kernel (src/cuda/kernel.cu:702-763).  Neighbour translations
+// are read from the pre-clustering snapshot (the reference updates them in
+// place while other threads read them).
+__global__ void cluster_kernel(ClusterArgs a) {
+  const float rot_sq = PPF_ROT_THRESH * PPF_ROT_THRESH;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < a.U;
+       i += (size_t)gridDim.x * blockDim.x) {
+    float3 t = make_float3(a.trans0[3 * i], a.trans0[3 * i + 1], a.trans0[3 * i + 2]);
+    float4 q = make_float4(a.quats[4 * i], a.quats[4 * i + 1], a.quats[4 * i + 2], a.quats[4 * i + 3]);
+    float c = 1;
+    float3 to = t;
+    for (int b = 0; b < 27; ++b) {
+      uint32_t key = a.adj[27 * i + b];
+      if (key == 0u) continue;
+      size_t lo = 0, hi = a.Kc;
+      while (lo < hi) {
+        size_t mid = (lo + hi) >> 1;
+        if (a.uniq[mid] < key) lo = mid + 1;
+        else hi = mid;
+      }
+      if (lo == a.Kc || a.uniq[lo] != key) continue;
+      uint32_t f = a.first[lo], cnt = a.count[lo];
+      for (uint32_t e = 0; e < cnt; ++e) {
+        uint32_t j = a.map[f + e];
+        float w = a.weighted[j];
+        float4 qj = make_float4(a.quats[4 * j], a.quats[4 * j + 1], a.quats[4 * j + 2], a.quats[4 * j + 3]);
+        float qd = fabsf(8 * (1 - dot4(q, qj)));
+        if (qd < rot_sq) {
+          float3 tj = make_float3(a.trans0[3 * j], a.trans0[3 * j + 1], a.trans0[3 * j + 2]);
+          if (!a.use_l1) {
+            float nd = norm3(v3_sub(t, tj));
+            if (!(nd < a.d_dist)) continue;
+          }
+          if (a.use_avg) {
+            to = v3_scale(c, to);
+            to = v3_add(to, v3_scale(w, tj));
+            to = v3_scale(1 / (c + w), to);
+          }
+          c += w;
+        }
+      }
+    }
+    a.scores[i] = c;
+    a.trans[3 * i] = to.x;
+    a.trans[3 * i + 1] = to.y;
+    a.trans[3 * i + 2] = to.z;
+  }
+}
+
+// First index of the largest score (thrust::max_element semantics), then the
+// pose assembly of ppf.cu:78-93 into best[0..15]; best[16] = score and
+// best[18..19] = index (uint64).
+__global__ void argmax_pose_kernel(const float* __restrict__ scores, size_t U,
+                                   const float* __restrict__ transforms,
+                                   const float* __restrict__ trans, float* __restrict__ best) {
+  __shared__ float s_v[32];
+  __shared__ unsigned long long s_i[32];
+  float bv = -INFINITY;
+  unsigned long long bi = ~0ull;
+  for (size_t i = threadIdx.x; i < U; i += blockDim.x) {
+    float v = scores[i];
+    if (v > bv || (v == bv && i < bi)) {
+      bv = v;
+      bi = i;
+    }
+  }
+  for (int o = 16; o; o >>= 1) {
+    float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+    unsigned long long oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (ov > bv || (ov == bv && oi < bi)) {
+      bv = ov;
+      bi = oi;
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    s_v[warp] = bv;
+    s_i[warp] = bi;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw = (blockDim.x + 31) / 32;
+    for (int w = 1; w < nw; ++w)
+      if (s_v[w] > bv || (s_v[w] == bv && s_i[w] < bi)) {
+        bv = s_v[w];
+        bi = s_i[w];
+      }
+    if (bi == ~0ull) bi = 0;  // all scores NaN: first element, as max_element
+    for (int k = 0; k < 16; ++k) best[k] = transforms[16 * bi + k];
+    best[3] = trans[3 * bi];
+    best[7] = trans[3 * bi + 1];
+    best[11] = trans[3 * bi + 2];
+    best[16] = scores[bi];
+    *reinterpret_cast<unsigned long long*>(best + 18) = bi;
+  }
+}
+
+template <typename T>
+T* grow(DevBuf& b, size_t n) {
+  b.reserve(n * sizeof(T));
+  return b.as<T>();
+}
+
+}  // namespace
+
+size_t select_votes(Context& ctx, const Model& m, const SceneData& s, LookupState& st,
+                    size_t n_cand, float min_votecount) {
+  cudaStream_t stream = ctx.stream;
+  unsigned long long* fcode = grow<unsigned long long>(st.tmp64, n_cand + 1);
+  uint32_t* fcount = grow<uint32_t>(st.tmp32a, n_cand + 1);
+  PPF_CUDA(cudaMemsetAsync(ctx.counters.ptr, 0, 4, stream));
+  filter_kernel<<<grid_for(n_cand, 256), 256, 0, stream>>>(
+      st.cand_codes.as<unsigned long long>(), st.cand_counts.as<uint32_t>(), n_cand, min_votecount,
+      fcode, fcount, ctx.counters.as<uint32_t>());
+  PPF_CUDA(cudaGetLastError());
+  ctx.launches++;
+  uint32_t U = 0;
+  PPF_CUDA(cudaMemcpyAsync(&U, ctx.counters.ptr, 4, cudaMemcpyDeviceToHost, stream));
+  PPF_CUDA(cudaStreamSynchronize(stream));
+  st.U = U;
+  if (U == 0) return 0;
+  // code ascending (codes are unique), counts carried as values
+  int end_bit = 33;
+  while (end_bit < 64 && ((unsigned long long)s.n >> (end_bit - 32)) != 0) ++end_bit;
+  PPF_CUDA(cudaMemsetAsync(ctx.flags.ptr, 0, 4, stream));
+  size_t l0 = ctx.sort64.launches() + ctx.sort32.launches();
+  ctx.sort64.sort(fcode, fcount, false, U, 0, end_bit, stream, ctx.flags.as<uint32_t>());
+  // then stable by count descending
+  uint32_t* key2 = grow<uint32_t>(st.tmp32b, U);
+  uint32_t* perm = grow<uint32_t>(st.perm, U);
+  count_key_kernel<<<grid_for(U, 256), 256, 0, stream>>>(fcount, U, key2);
+  ctx.sort32.sort(key2, perm, true, U, 0, 32, stream, ctx.flags.as<uint32_t>());
+  gather_kernel<<<grid_for(U, 256), 256, 0, stream>>>(perm, fcode, fcount, U,
+                                                       grow<unsigned long long>(st.codes, U),
+                                                       grow<uint32_t>(st.counts, U));
+  PPF_CUDA(cudaGetLastError());
+  ctx.launches += 2 + (ctx.sort64.launches() + ctx.sort32.launches() - l0);
+  return U;
+}
+
+void sort_by_code(Context& ctx, LookupState& st, size_t n) {
+  if (n == 0) return;
+  cudaStream_t stream = ctx.stream;
+  unsigned long long* code = grow<unsigned long long>(st.codes, n);
+  uint32_t* count = grow<uint32_t>(st.counts, n);
+  PPF_CUDA(cudaMemcpyAsync(code, st.cand_codes.ptr, n * 8, cudaMemcpyDeviceToDevice, stream));
+  PPF_CUDA(cudaMemcpyAsync(count, st.cand_counts.ptr, n * 4, cudaMemcpyDeviceToDevice, stream));
+  PPF_CUDA(cudaMemsetAsync(ctx.flags.ptr, 0, 4, stream));
+  size_t l0 = ctx.sort64.launches();
+  ctx.sort64.sort(code, count, false, n, 0, 64, stream, ctx.flags.as<uint32_t>());
+  ctx.launches += ctx.sort64.launches() - l0;
+}
+
+void compute_poses(Context& ctx, const Model& m, const SceneData& s, LookupState& st) {
+  const size_t U = st.U;
+  cudaStream_t stream = ctx.stream;
+  PoseArgs a;
+  a.codes = st.codes.as<unsigned long long>();
+  a.counts = st.counts.as<uint32_t>();
+  a.U = U;
+  a.m_pts = m.t.pts.as<float4>();
+  a.m_ang = m.t.angles.as<float2>();
+  a.m_w = m.t.weights.as<float>();
+  a.s_pts = s.pts.as<float4>();
+  a.s_nrm = s.nrm.as<float4>();
+  a.d_dist = m.t.d_dist;
+  a.transforms = grow<float>(st.transforms, U * 16);
+  a.trans0 = grow<float>(st.trans0, U * 3);
+  a.quats = grow<float>(st.quats, U * 4);
+  a.weighted = grow<float>(st.weighted, U);
+  a.cell_keys = grow<uint32_t>(st.cell_keys, U);
+  a.adj = grow<uint32_t>(st.adj, U * 27);
+  grow<float>(st.trans, U * 3);
+  grow<float>(st.scores, U);
+  if (U <= 1) {
+    // Every per-vote kernel of the reference returns early when its count is
+    // <= 1 (src/cuda/kernel.cu:609,651,667,712,769): a single kept vote leaves
+    // zero transforms, zero scores and an all-zero pose.
+    PPF_CUDA(cudaMemsetAsync(a.transforms, 0, U * 64, stream));
+    PPF_CUDA(cudaMemsetAsync(a.trans0, 0, U * 12, stream));
+    PPF_CUDA(cudaMemsetAsync(st.trans.ptr, 0, U * 12, stream));
+    PPF_CUDA(cudaMemsetAsync(a.quats, 0, U * 16, stream));
+    PPF_CUDA(cudaMemsetAsync(a.weighted, 0, U * 4, stream));
+    PPF_CUDA(cudaMemsetAsync(a.cell_keys, 0, U * 4, stream));
+    PPF_CUDA(cudaMemsetAsync(st.scores.ptr, 0, U * 4, stream));
+    return;
+  }
+  poses_kernel<<<grid_for(U, 128), 128, 0, stream>>>(a);
+  PPF_CUDA(cudaGetLastError());
+  ctx.launches++;
+}
+
+size_t cluster_poses_gpu(Context& ctx, const Model& m, LookupState& st, float* best_score) {
+  const size_t U = st.U;
+  cudaStream_t stream = ctx.stream;
+  float* best = grow<float>(st.best, 32);
+  if (U <= 1) {
+    PPF_CUDA(cudaMemsetAsync(best, 0, 32 * sizeof(float), stream));
+    *best_score = 0;
+    return 0;
+  }
+  // hash array of the pose cells (src/cuda/model.cu:222-226)
+  uint32_t* ck = grow<uint32_t>(st.cells_sorted, U);
+  uint32_t* map = grow<uint32_t>(st.cells_map, U);
+  PPF_CUDA(cudaMemcpyAsync(ck, st.cell_keys.ptr, U * 4, cudaMemcpyDeviceToDevice, stream));
+  PPF_CUDA(cudaMemsetAsync(ctx.flags.ptr, 0, 4, stream));
+  size_t l0 = ctx.sort32.launches();
+  ctx.sort32.sort(ck, map, true, U, 0, 32, stream, ctx.flags.as<uint32_t>());
+  ctx.launches += ctx.sort32.launches() - l0;
+  uint32_t* uq = grow<uint32_t>(st.cells_uniq, U);
+  uint32_t* fi = grow<uint32_t>(st.cells_first, U);
+  uint32_t* ct = grow<uint32_t>(st.cells_count, U);
+  size_t Kc = build_runs(ck, U, uq, fi, ct, ctx.scratch, stream, &ctx.launches);
+  ClusterArgs a;
+  a.U = U;
+  a.trans0 = st.trans0.as<float>();
+  a.quats = st.quats.as<float>();
+  a.weighted = st.weighted.as<float>();
+  a.adj = st.adj.as<uint32_t>();
+  a.uniq = uq;
+  a.first = fi;
+  a.count = ct;
+  a.map = map;
+  a.Kc = Kc;
+  a.d_dist = m.t.d_dist;
+  a.use_l1 = m.use_l1_norm;
+  a.use_avg = m.use_averaged_clusters;
+  a.scores = st.scores.as<float>();
+  a.trans = st.trans.as<float>();
+  cluster_kernel<<<grid_for(U, 128), 128, 0, stream>>>(a);
+  argmax_pose_kernel<<<1, 1024, 0, stream>>>(a.scores, U, st.transforms.as<float>(), a.trans, best);
+  PPF_CUDA(cudaGetLastError());
+  ctx.launches += 2;
+  float h[20];
+  PPF_CUDA(cudaMemcpyAsync(h, best, sizeof(h), cudaMemcpyDeviceToHost, stream));
+  PPF_CUDA(cudaStreamSynchronize(stream));
+  *best_score = h[16];
+  unsigned long long idx;
+  memcpy(&idx, h + 18, sizeof(idx));
+  return (size_t)idx;
+}
+
+}  // namespace ppf

@@ -1,0 +1,41 @@
+// Device-wide primitives written for this engine: a stable LSD radix sort of
+// (key, uint32 value) pairs and run-table construction over sorted keys.
+#pragma once
+
+#include "common.cuh"
+
+namespace ppf {
+
+// Stable LSD radix sort, 8-bit digits, one "onesweep" kernel per digit:
+// each tile ranks its keys with warp multisplit, publishes per-digit counts
+// and resolves its global offsets by decoupled look-back over the preceding
+// tiles (tiles are numbered in launch order through an atomic counter, so
+// every tile it waits on is already resident).  Waits are bounded; a wait
+// that gives up raises kFlagSpinTimeout in *flags.
+//
+// keys/vals hold the input and receive the output (n elements each);
+// vals == nullptr is not allowed, vals_iota makes the input values 0..n-1
+// (vals is then output-only).  Digits [begin_bit, end_bit) are sorted; bits
+// outside that range must not matter to the caller's order.
+template <typename K>
+class RadixSorter {
+ public:
+  void sort(K* keys, uint32_t* vals, bool vals_iota, size_t n, int begin_bit, int end_bit,
+            cudaStream_t st, uint32_t* d_flags);
+  size_t launches() const { return launches_; }
+
+ private:
+  DevBuf kalt_, valt_, hist_, status_, counters_;
+  size_t launches_ = 0;
+};
+
+extern template class RadixSorter<uint32_t>;
+extern template class RadixSorter<unsigned long long>;
+
+// Run table of a sorted key array: K unique keys, the first position of each
+// run and its length.  Returns K (synchronises the stream once to read it).
+// uniq/first/count must have room for n entries.
+size_t build_runs(const uint32_t* sorted_keys, size_t n, uint32_t* uniq, uint32_t* first,
+                  uint32_t* count, DevBuf& scratch, cudaStream_t st, size_t* launches);
+
+}  // namespace ppf

@@ -1,0 +1,411 @@
+// The vote pass: the work of Scene::Scene + Model::ComputeUniqueVotes
+// (src/cuda/scene.cu:24-55, src/cuda/model.cu:95-171) without materialising
+// scene pair features or individual votes.
+//
+// One work item = (scene reference point s_r, chunk of model reference points).
+// A persistent block takes items from an atomic counter.  For its s_r it walks
+// all scene points in tiles of 512: each thread computes one pair feature, its
+// FNV key, and looks the key up in the model's key -> run table; matched pairs
+// are queued in shared memory with their sub-run for this chunk.  The block
+// then spreads the queued votes evenly over its warps (consecutive lanes read
+// consecutive run entries) and counts each vote into a shared-memory
+// accumulator of (m_r, alpha bin) cells.  When the item is done, the block
+// folds its largest count into a global running maximum and emits every cell
+// whose count exceeds threshold x running maximum: a superset of the cells
+// the final threshold (threshold x global maximum) keeps.
+#include "engine.h"
+#include "ppf_math.cuh"
+
+namespace ppf {
+namespace {
+
+constexpr int kUnroll = 8;
+constexpr int kUnit = 32 * kUnroll;
+
+struct VoteArgs {
+  // model
+  const uint32_t* entries;
+  const uint32_t* pairs;
+  const uint32_t* split;
+  const uint32_t* run_count;
+  const uint8_t* run_flags;
+  const uint32_t* ht_keys;
+  const uint32_t* ht_runs;
+  uint32_t ht_mask;
+  const float4* m_r1;
+  const float4* m_r2;
+  const float4* m_pts;
+  uint32_t n_m, chunk, n_chunks;
+  // scene
+  const float4* s_pts;
+  const float4* s_nrm;
+  uint32_t n_s, ref_df, n_ref, perm_mul;
+  float d_dist, thr, floor;
+  int emit_all;
+  // control / outputs
+  uint32_t n_items;
+  uint32_t* work_counter;
+  uint32_t* global_max;
+  unsigned long long* stats;  // [0] votes, [1] matched pairs, [2] exact bins
+  unsigned long long* cand_code;
+  uint32_t* cand_count;
+  uint32_t* n_cand;
+  uint32_t cand_cap;
+  uint32_t* flags;
+};
+
+__device__ __forceinline__ uint32_t ht_lookup(const uint32_t* __restrict__ keys,
+                                              const uint32_t* __restrict__ runs, uint32_t mask,
+                                              uint32_t key) {
+  uint32_t s = (key * 0x9E3779B1u) & mask;
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    uint32_t k = __ldg(keys + s);
+    if (k == key) return __ldg(runs + s);
+    if (k == 0u) return 0xffffffffu;
+    s = (s + 1) & mask;
+  }
+  return 0xffffffffu;
+}
+
+__device__ __forceinline__ uint32_t block_excl_scan512(uint32_t v, uint32_t* s_warp,
+                                                       uint32_t* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < kVoteWarps ? s_warp[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < kVoteWarps) s_warp[lane] = w;
+  }
+  __syncthreads();
+  uint32_t r = (warp ? s_warp[warp - 1] : 0u) + x - v;
+  if (total) *total = s_warp[kVoteWarps - 1];
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  const uint32_t cells = a.chunk * kBins;
+  uint32_t* acc = smem;
+  uint32_t* q_off = acc + ((cells + 3u) & ~3u);  // kVoteThreads + 1
+  uint32_t* q_lo = q_off + kVoteThreads + 4;
+  uint32_t* q_beta = q_lo + kVoteThreads;
+  float2* q_v = reinterpret_cast<float2*>(q_beta + kVoteThreads);
+
+  __shared__ uint32_t s_item, s_total, s_max;
+  __shared__ uint32_t s_warp[kVoteWarps];
+  __shared__ float4 s_fr[2];  // scene frame rows 1, 2
+  __shared__ float4 s_pr, s_nr;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  unsigned long long my_votes = 0, my_matched = 0, my_exact = 0;
+
+  for (;;) {
+    if (tid == 0) s_item = atomicAdd(a.work_counter, 1u);
+    __syncthreads();
+    const uint32_t item = s_item;
+    if (item >= a.n_items) break;
+    const uint32_t c = item % a.n_chunks;
+    const uint32_t ref = (uint32_t)(((unsigned long long)(item / a.n_chunks) * a.perm_mul) % a.n_ref);
+    const uint32_t sr = ref * a.ref_df;
+    const uint32_t mr_base = c * a.chunk;
+    if (tid == 0) {
+      float4 p = a.s_pts[sr], q = a.s_nrm[sr];
+      FrameYZ f = frame_yz(make_float3(p.x, p.y, p.z), make_float3(q.x, q.y, q.z));
+      s_fr[0] = f.r1;
+      s_fr[1] = f.r2;
+      s_pr = p;
+      s_nr = q;
+    }
+    for (uint32_t i = tid; i < cells; i += kVoteThreads) acc[i] = 0u;
+    __syncthreads();
+    const float3 pr = make_float3(s_pr.x, s_pr.y, s_pr.z);
+    const float3 nr = make_float3(s_nr.x, s_nr.y, s_nr.z);
+    FrameYZ fs;
+    fs.r1 = s_fr[0];
+    fs.r2 = s_fr[1];
+
+    for (uint32_t base = 0; base < a.n_s; base += kVoteThreads) {
+      // ---- one scene pair per thread: feature, key, lookup, sub-run
+      const uint32_t i = base + tid;
+      uint32_t len = 0, lo = 0, beta = 0;
+      float2 v = make_float2(0.f, 0.f);
+      if (i < a.n_s && i != sr) {
+        float4 pi4 = a.s_pts[i], ni4 = a.s_nrm[i];
+        float3 pi = make_float3(pi4.x, pi4.y, pi4.z);
+        float4 f = pair_feature(pr, nr, pi, make_float3(ni4.x, ni4.y, ni4.z), a.d_dist);
+        uint32_t key = feature_key(f);
+        if (key != 0u) {
+          uint32_t run = ht_lookup(a.ht_keys, a.ht_runs, a.ht_mask, key);
+          if (run != 0xffffffffu) {
+            const uint32_t* sp = a.split + (size_t)run * (a.n_chunks + 1);
+            lo = __ldg(sp + c);
+            len = __ldg(sp + c + 1) - lo;
+            if (c == 0) {
+              my_votes += __ldg(a.run_count + run);
+              my_matched += 1;
+            }
+            if (len) {
+              v = frame_point_yz(fs, pi);
+              bool degenerate = fabsf(v.x) + fabsf(v.y) < 1e-12f || !isfinite(v.x) || !isfinite(v.y);
+              beta = angle16(v) | ((degenerate || __ldg(a.run_flags + run)) ? 0x10000u : 0u);
+            }
+          }
+        }
+      }
+      uint32_t total;
+      uint32_t off = block_excl_scan512(len, s_warp, &total);
+      q_off[tid] = off;
+      q_lo[tid] = lo;
+      q_beta[tid] = beta;
+      q_v[tid] = v;
+      if (tid == 0) q_off[kVoteThreads] = total;
+      __syncthreads();
+
+      // ---- spread the tile's votes over the warps
+      for (uint32_t ustart = (uint32_t)warp * kUnit; ustart < total; ustart += kVoteWarps * kUnit) {
+        uint32_t plo = 0, phi = kVoteThreads;
+        while (phi - plo > 1) {
+          uint32_t mid = (plo + phi) >> 1;
+          if (q_off[mid] <= ustart) plo = mid;
+          else phi = mid;
+        }
+        uint32_t p = plo;
+        uint32_t nxt = q_off[p + 1];
+        uint32_t pbase = q_lo[p] - q_off[p];
+        uint32_t pbeta = q_beta[p];
+        uint32_t pos[kUnroll], bs[kUnroll], pk[kUnroll], ent[kUnroll];
+#pragma unroll
+        for (int k = 0; k < kUnroll; ++k) {
+          uint32_t vi = ustart + lane + 32u * k;
+          pos[k] = 0xffffffffu;
+          if (vi < total) {
+            if (vi >= nxt) {
+              do {
+                ++p;
+                nxt = q_off[p + 1];
+              } while (vi >= nxt);
+              pbase = q_lo[p] - q_off[p];
+              pbeta = q_beta[p];
+            }
+            pos[k] = pbase + vi;
+            bs[k] = pbeta;
+            pk[k] = p;
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < kUnroll; ++k)
+          if (pos[k] != 0xffffffffu) ent[k] = __ldg(a.entries + pos[k]);
+#pragma unroll
+        for (int k = 0; k < kUnroll; ++k) {
+          if (pos[k] == 0xffffffffu) continue;
+          const uint32_t mr = ent[k] >> 16;
+          int bin = (bs[k] & 0x10000u) ? -1 : alpha_bin_fast(ent[k] & 0xffffu, bs[k] & 0xffffu);
+          if (bin < 0) {
+            // exact path: the reference's own arithmetic for this vote
+            const uint32_t pr_idx = __ldg(a.pairs + pos[k]);
+            const uint32_t mi = pr_idx - mr * a.n_m;
+            FrameYZ fm;
+            fm.r1 = __ldg(a.m_r1 + mr);
+            fm.r2 = __ldg(a.m_r2 + mr);
+            float4 q4 = __ldg(a.m_pts + mi);
+            float2 u = frame_point_yz(fm, make_float3(q4.x, q4.y, q4.z));
+            bin = (int)alpha_bin_exact(u, q_v[pk[k]]);
+            ++my_exact;
+          }
+          atomicAdd(&acc[(mr - mr_base) * kBins + (uint32_t)bin], 1u);
+        }
+      }
+      __syncthreads();
+    }
+
+    // ---- fold the item's maximum into the running maximum, emit cells
+    uint32_t lmax = 0;
+    for (uint32_t i = tid; i < cells; i += kVoteThreads) lmax = max(lmax, acc[i]);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) lmax = max(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+    if (lane == 0) s_warp[warp] = lmax;
+    __syncthreads();
+    if (tid == 0) {
+      uint32_t m = 0;
+      for (int w = 0; w < kVoteWarps; ++w) m = max(m, s_warp[w]);
+      uint32_t old = atomicMax(a.global_max, m);
+      s_max = max(old, m);
+    }
+    __syncthreads();
+    const float floor_v = a.floor >= 0.f ? a.floor : a.thr * (float)s_max;
+    for (uint32_t b0 = 0; b0 < cells; b0 += kVoteThreads) {
+      const uint32_t cell = b0 + tid;
+      uint32_t cnt = cell < cells ? acc[cell] : 0u;
+      bool keep = cnt != 0u && (a.emit_all || (float)cnt > floor_v);
+      uint32_t ballot = __ballot_sync(0xffffffffu, keep);
+      if (!ballot) continue;
+      uint32_t slot0 = 0;
+      if (lane == 0) slot0 = atomicAdd(a.n_cand, (uint32_t)__popc(ballot));
+      slot0 = __shfl_sync(0xffffffffu, slot0, 0);
+      if (keep) {
+        uint32_t slot = slot0 + __popc(ballot & ((1u << lane) - 1u));
+        if (slot < a.cand_cap) {
+          uint32_t mr = mr_base + cell / kBins, bin = cell % kBins;
+          a.cand_code[slot] = ((unsigned long long)sr << 32) | ((unsigned long long)mr << 6) | bin;
+          a.cand_count[slot] = cnt;
+        } else {
+          atomicOr(a.flags, (uint32_t)kFlagCandidateOverflow);
+        }
+      }
+    }
+    __syncthreads();
+  }
+
+  // per-block statistics
+  for (int o = 16; o; o >>= 1) {
+    my_votes += __shfl_xor_sync(0xffffffffu, my_votes, o);
+    my_matched += __shfl_xor_sync(0xffffffffu, my_matched, o);
+    my_exact += __shfl_xor_sync(0xffffffffu, my_exact, o);
+  }
+  if (lane == 0) {
+    if (my_votes) atomicAdd(&a.stats[0], my_votes);
+    if (my_matched) atomicAdd(&a.stats[1], my_matched);
+    if (my_exact) atomicAdd(&a.stats[2], my_exact);
+  }
+}
+
+// counts[r * n_s + i]: model run length of a matching scene pair (r, i).
+__global__ void pair_vote_counts_kernel(VoteArgs a, unsigned long long* __restrict__ out) {
+  for (uint32_t r = blockIdx.y; r < a.n_s; r += gridDim.y) {
+    unsigned long long* row = out + (size_t)r * a.n_s;
+    const bool ref_row = (r % a.ref_df) == 0 && a.n_s > 1;
+    float4 p4 = a.s_pts[r], n4 = a.s_nrm[r];
+    float3 pr = make_float3(p4.x, p4.y, p4.z), nr = make_float3(n4.x, n4.y, n4.z);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_s;
+         i += gridDim.x * blockDim.x) {
+      unsigned long long cnt = 0;
+      if (ref_row && i != r) {
+        float4 q4 = a.s_pts[i], m4 = a.s_nrm[i];
+        float4 f = pair_feature(pr, nr, make_float3(q4.x, q4.y, q4.z),
+                                make_float3(m4.x, m4.y, m4.z), a.d_dist);
+        uint32_t key = feature_key(f);
+        if (key) {
+          uint32_t run = ht_lookup(a.ht_keys, a.ht_runs, a.ht_mask, key);
+          if (run != 0xffffffffu) cnt = a.run_count[run];
+        }
+      }
+      row[i] = cnt;
+    }
+  }
+}
+
+uint32_t gcd_u32(uint32_t x, uint32_t y) {
+  while (y) {
+    uint32_t t = x % y;
+    x = y;
+    y = t;
+  }
+  return x;
+}
+
+VoteArgs make_args(const Model& m, const SceneData& s) {
+  const ModelTables& t = m.t;
+  VoteArgs a{};
+  a.entries = t.entries.as<uint32_t>();
+  a.pairs = t.pairs.as<uint32_t>();
+  a.split = t.split.as<uint32_t>();
+  a.run_count = t.count.as<uint32_t>();
+  a.run_flags = t.run_flags.as<uint8_t>();
+  a.ht_keys = t.ht_keys.as<uint32_t>();
+  a.ht_runs = t.ht_runs.as<uint32_t>();
+  a.ht_mask = t.ht_mask;
+  a.m_r1 = t.frame_r1.as<float4>();
+  a.m_r2 = t.frame_r2.as<float4>();
+  a.m_pts = t.pts.as<float4>();
+  a.n_m = t.n;
+  a.chunk = t.chunk;
+  a.n_chunks = t.n_chunks;
+  a.s_pts = s.pts.as<float4>();
+  a.s_nrm = s.nrm.as<float4>();
+  a.n_s = s.n;
+  a.ref_df = s.ref_df ? s.ref_df : 1;
+  a.n_ref = (s.n + a.ref_df - 1) / a.ref_df;
+  a.d_dist = s.d_dist;  // scene pair features use the scene's quantum
+  a.thr = m.vote_count_threshold;
+  // ref visiting order: j -> j * perm_mul mod n_ref (a bijection)
+  uint32_t pm = a.n_ref > 1 ? (0x9E3779B1u % a.n_ref) : 1u;
+  if (pm == 0) pm = 1;
+  while (a.n_ref > 1 && gcd_u32(pm, a.n_ref) != 1) ++pm;
+  a.perm_mul = pm;
+  return a;
+}
+
+}  // namespace
+
+VoteResult run_votes(Context& ctx, const Model& m, const SceneData& s, LookupState& st,
+                     bool emit_all, float floor, size_t cand_cap) {
+  VoteResult r;
+  cudaStream_t stream = ctx.stream;
+  VoteArgs a = make_args(m, s);
+  a.emit_all = emit_all ? 1 : 0;
+  a.floor = floor;
+  a.n_items = a.n_ref * a.n_chunks;
+  if (s.n < 2 || a.n_items == 0) return r;
+  // counters: [0] work, [1] max, [2] n_cand, [3] pad, then 3 x u64 stats
+  ctx.counters.reserve(64);
+  PPF_CUDA(cudaMemsetAsync(ctx.counters.ptr, 0, 64, stream));
+  PPF_CUDA(cudaMemsetAsync(ctx.flags.ptr, 0, sizeof(uint32_t), stream));
+  uint32_t* cnt = ctx.counters.as<uint32_t>();
+  a.work_counter = cnt + 0;
+  a.global_max = cnt + 1;
+  a.n_cand = cnt + 2;
+  a.stats = reinterpret_cast<unsigned long long*>(cnt + 4);
+  a.flags = ctx.flags.as<uint32_t>();
+  st.cand_codes.reserve(cand_cap * sizeof(unsigned long long));
+  st.cand_counts.reserve(cand_cap * sizeof(uint32_t));
+  a.cand_code = st.cand_codes.as<unsigned long long>();
+  a.cand_count = st.cand_counts.as<uint32_t>();
+  a.cand_cap = (uint32_t)cand_cap;
+
+  const uint32_t cells = a.chunk * kBins;
+  size_t smem = (size_t)((cells + 3u) & ~3u) * 4 + (kVoteThreads + 4) * 4 + kVoteThreads * 4 * 2 +
+                kVoteThreads * 8;
+  PPF_REQUIRE((int)smem <= ctx.vote_smem_limit, PPF_ERR_INTERNAL, "vote accumulator too large");
+  PPF_CUDA(cudaFuncSetAttribute(vote_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  unsigned grid = (unsigned)std::min<size_t>(a.n_items, (size_t)sm_count());
+  PPF_CUDA(cudaEventRecord(ctx.ev[0], stream));
+  vote_kernel<<<grid, kVoteThreads, smem, stream>>>(a);
+  PPF_CUDA(cudaGetLastError());
+  PPF_CUDA(cudaEventRecord(ctx.ev[1], stream));
+  ctx.launches++;
+  uint32_t h[16];
+  PPF_CUDA(cudaMemcpyAsync(h, ctx.counters.ptr, 64, cudaMemcpyDeviceToHost, stream));
+  uint32_t flags = 0;
+  PPF_CUDA(cudaMemcpyAsync(&flags, ctx.flags.ptr, 4, cudaMemcpyDeviceToHost, stream));
+  PPF_CUDA(cudaStreamSynchronize(stream));
+  PPF_CUDA(cudaEventElapsedTime(&r.vote_ms, ctx.ev[0], ctx.ev[1]));
+  r.max_count = h[1];
+  r.n_cand = h[2];
+  unsigned long long* s64 = reinterpret_cast<unsigned long long*>(h + 4);
+  r.n_votes = s64[0];
+  r.n_matched = s64[1];
+  r.n_exact = s64[2];
+  return r;
+}
+
+void pair_vote_counts(Context& ctx, const Model& m, const SceneData& s, uint64_t* out_dev) {
+  VoteArgs a = make_args(m, s);
+  dim3 grid((s.n + 255) / 256, std::min<uint32_t>(s.n, 65535u));
+  pair_vote_counts_kernel<<<grid, 256, 0, ctx.stream>>>(a, reinterpret_cast<unsigned long long*>(out_dev));
+  PPF_CUDA(cudaGetLastError());
+  ctx.launches++;
+}
+
+}  // namespace ppf

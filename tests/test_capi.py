@@ -1,0 +1,60 @@
+"""C ABI: the library loads, exports every declared symbol, and reports
+argument errors as statuses (no GPU needed, no compute calls)."""
+import ctypes as C
+import subprocess
+
+import pytest
+
+
+def test_library_exports_every_header_symbol(pkg):
+    from importlib import import_module
+
+    capi = import_module("ppf_b200._capi")
+    lib = capi.load()
+    syms = capi.header_symbols()
+    assert len(syms) >= 20
+    missing = [s for s in syms if not hasattr(lib, s)]
+    assert not missing, missing
+    out = subprocess.run(["nm", "-D", "--defined-only", str(capi.LIBPATH)], capture_output=True, text=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if " T " in line}
+    assert set(syms) <= exported
+    # every declared symbol has a ctypes signature
+    assert set(syms) == set(capi.SIGNATURES)
+
+
+def test_abi_version_and_error_text(pkg):
+    lib = pkg.load()
+    assert lib.ppf_abi_version() == 1
+    assert lib.ppf_last_error() is not None
+
+
+def test_null_handles_are_invalid_arguments(pkg):
+    lib = pkg.load()
+    h = C.c_void_p()
+    assert lib.ppf_model_create(None, None, None, 0, 0.01, 0.3, 0, 0, 0, C.byref(h)) == 1
+    assert b"null" in lib.ppf_last_error()
+    assert lib.ppf_scene_create(None, None, None, 0, 0.01, 1, C.byref(h)) == 1
+    assert lib.ppf_model_lookup(None, None, None, None) == 1
+    n = C.c_uint64()
+    assert lib.ppf_model_get_votes(None, None, None, 0, C.byref(n)) == 1
+    # destroy of a null handle is a no-op
+    assert lib.ppf_model_destroy(None) == 0
+    assert lib.ppf_scene_destroy(None) == 0
+    assert lib.ppf_context_destroy(None) == 0
+
+
+def test_header_is_plain_c():
+    from pathlib import Path
+
+    hdr = Path(__file__).resolve().parents[1] / "include" / "ppf_b200.h"
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-fsyntax-only", "-x", "c", str(hdr)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
+def test_missing_library_fails_loudly(pkg, tmp_path):
+    from importlib import import_module
+
+    capi = import_module("ppf_b200._capi")
+    with pytest.raises(RuntimeError, match="missing"):
+        capi.load(tmp_path / "nope.so")

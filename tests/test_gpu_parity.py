@@ -1,0 +1,253 @@
+"""GPU parity: the engine against the reference's own CUDA kernels.
+
+The reference kernels (src/cuda/kernel.cu, built in place for sm_100a with the
+reference's arithmetic flags into oracle/_ref/libppfref_gpu.so) run on the same
+B200 in model.cu order and are the bit-exact oracle for all integer work:
+feature keys, the model hash array, per-scene-pair vote counts, every
+(s_r, m_r, alpha) vote count, the threshold and its order.  Float outputs
+derived from those integers (poses, quaternions, clustering scores) are
+compared bit for bit as well (NaN == NaN), except the averaged-cluster
+translations, where the reference races (src/cuda/kernel.cu:747-758) and the
+tolerance is 1e-5 x model diameter.  Sizes are kept small enough that the
+reference, which materialises every vote, finishes in seconds.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _same(a, b):
+    a = np.asarray(a, np.float32)
+    b = np.asarray(b, np.float32)
+    return a.shape == b.shape and bool(np.all((a.view(np.uint32) == b.view(np.uint32)) | (np.isnan(a) & np.isnan(b))))
+
+
+CASES = {
+    # name: (seed, n_model, n_plane, n_box, ref_df, thr)
+    "small": (31, 300, 500, 200, 5, 0.3),
+    "medium": (32, 700, 1500, 500, 5, 0.3),
+    "df1": (33, 250, 300, 150, 1, 0.4),
+}
+
+
+@pytest.fixture(scope="module", params=list(CASES))
+def case(request, pkg):
+    seed, nm, npl, nb, df, thr = CASES[request.param]
+    spec = pkg.synthetic.config_plain(seed=seed, n_model=nm, n_plane=npl, n_box=nb, ref_point_df=df,
+                                      vote_count_threshold=thr)
+    return request.param, spec
+
+
+def _mk(pkg, ctx, spec, **kw):
+    m, s, d = spec.models[0], spec.scene, spec.d_dists[0]
+    model = pkg.Model(m, d, spec.vote_count_threshold, context=ctx, **kw)
+    scene = pkg.Scene(s, d, spec.ref_point_df, context=ctx)
+    return model, scene
+
+
+def test_pair_keys_bit_exact(pkg, ctx, ref_gpu, case):
+    _, spec = case
+    for cloud, df in ((spec.models[0], 1), (spec.scene, spec.ref_point_df)):
+        mine = pkg.pair_keys(cloud, spec.d_dists[0], df, context=ctx)
+        ref = ref_gpu.pair_keys(cloud.points, cloud.normals, spec.d_dists[0], df)
+        assert np.array_equal(mine, ref)
+
+
+def test_model_hash_array_bit_exact(pkg, ctx, ref_gpu, case):
+    _, spec = case
+    model, _ = _mk(pkg, ctx, spec)
+    H = model.hash_array()
+    R = ref_gpu.model_tables(spec.models[0].points, spec.models[0].normals, spec.d_dists[0])
+    for k in ("keys", "counts", "first", "map"):
+        assert np.array_equal(H[k], R[k]), k
+
+
+def test_vote_counts_and_all_votes_bit_exact(pkg, ctx, ref_gpu, case):
+    _, spec = case
+    model, scene = _mk(pkg, ctx, spec)
+    R = ref_gpu.lookup((spec.models[0].points, spec.models[0].normals), (spec.scene.points, spec.scene.normals),
+                       spec.d_dists[0], spec.ref_point_df, spec.vote_count_threshold, all_votes=True,
+                       pair_counts=True)
+    assert np.array_equal(model.pair_vote_counts(scene), R["pair_counts"])
+    codes, counts = model.all_votes(scene)
+    assert codes.size == R["n_unique"]
+    assert np.array_equal(codes, R["all_codes"])
+    assert np.array_equal(counts, R["all_counts"])
+
+
+def test_lookup_bit_exact(pkg, ctx, ref_gpu, case):
+    _, spec = case
+    model, scene = _mk(pkg, ctx, spec)
+    pose = model.ppf_lookup(scene)
+    R = ref_gpu.lookup((spec.models[0].points, spec.models[0].normals), (spec.scene.points, spec.scene.normals),
+                       spec.d_dists[0], spec.ref_point_df, spec.vote_count_threshold)
+    st = model.stats
+    assert st["n_votes"] == R["n_votes"]
+    assert st["max_vote_count"] == R["max_count"]
+    assert st["n_kept"] == R["n_kept"]
+    codes, counts = model.get_votes()
+    assert np.array_equal(codes, R["codes"]) and np.array_equal(counts, R["counts"])
+    assert _same(model.getTransformations(), R["transforms"])
+    t, q, s = model.get_cluster_state()
+    assert _same(q, R["quats"])
+    assert _same(s, R["scores"])
+    assert _same(t, R["trans"])
+    assert st["max_idx"] == R["max_idx"]
+    assert _same(pose.ravel(), R["pose"].ravel())
+
+
+@pytest.mark.parametrize("mode", ["l1", "avg", "weights"])
+def test_lookup_modes(pkg, ctx, ref_gpu, mode):
+    spec = pkg.synthetic.config_plain(seed=41, n_model=400, n_plane=700, n_box=300)
+    kw = {"use_l1_norm": mode == "l1", "use_averaged_clusters": mode == "avg"}
+    model, scene = _mk(pkg, ctx, spec, **kw)
+    w = None
+    if mode == "weights":
+        w = np.random.default_rng(0).uniform(0.5, 2.0, len(spec.models[0])).astype(np.float32)
+        model.SetModelPointVoteWeights(w)
+    pose = model.ppf_lookup(scene)
+    R = ref_gpu.lookup((spec.models[0].points, spec.models[0].normals), (spec.scene.points, spec.scene.normals),
+                       spec.d_dists[0], spec.ref_point_df, spec.vote_count_threshold, weights=w, **kw)
+    codes, counts = model.get_votes()
+    assert np.array_equal(codes, R["codes"]) and np.array_equal(counts, R["counts"])
+    t, q, s = model.get_cluster_state()
+    if mode == "avg":
+        # the reference reads neighbour translations while other threads
+        # overwrite them; scores are unaffected, translations agree to 1e-5 diam
+        assert _same(s, R["scores"])
+        tol = 1e-5 * spec.diameters[0]
+        assert np.max(np.abs(t - R["trans"])) <= tol
+        assert np.max(np.abs(pose[:3, 3] - R["pose"][:3, 3])) <= tol
+        assert _same(pose[:3, :3], R["pose"][:3, :3])
+    else:
+        # float sums of weights may round differently in another order;
+        # integer weights (the reference's case) are exact
+        if mode == "weights":
+            assert np.allclose(s, R["scores"], rtol=1e-6)
+        else:
+            assert _same(s, R["scores"])
+        assert _same(pose.ravel(), R["pose"].ravel())
+
+
+def test_keys_against_cpu_oracle(pkg, ctx, oracle):
+    """CPU libm and IEEE division vs the device's fast-math: keys agree except
+    at quantisation boundaries (stated flip rate < 1e-3)."""
+    spec = pkg.synthetic.config_plain(seed=51, n_model=800, n_plane=10, n_box=10)
+    m, d = spec.models[0], spec.d_dists[0]
+    gpu = pkg.pair_keys(m, d, 1, context=ctx)
+    cpu = oracle.pair_keys(m.points, m.normals, d)
+    flips = float(np.mean(gpu != cpu))
+    assert flips < 1e-3, flips
+
+
+def test_pose_against_fp64_and_ground_truth(pkg, ctx, oracle):
+    spec = pkg.synthetic.config_plain(seed=1000)
+    m, s, d = spec.models[0], spec.scene, spec.d_dists[0]
+    model = pkg.Model(m, d, 0.3, context=ctx)
+    scene = pkg.Scene(s, d, 5, context=ctx)
+    pose = model.ppf_lookup(scene)
+    codes, _ = model.get_votes()
+    code = int(codes[model.max_idx])
+    sr, mr, b = code >> 32, (code & 0xFFFFFFFF) >> 6, code & 63
+    T64 = oracle.vote_pose(b, m.points[mr], m.normals[mr], s.points[sr], s.normals[sr], f64=True)
+    T32 = model.getTransformations()[model.max_idx].reshape(4, 4)
+    assert np.max(np.abs(T32[:3, :3] - T64[:3, :3])) < 1e-4
+    assert np.max(np.abs(T32[:3, 3] - T64[:3, 3])) < 1e-5 * spec.diameters[0] * 10
+    G = spec.instances[0].pose
+    assert np.linalg.norm(pose[:3, 3] - G[:3, 3]) < 0.1 * spec.diameters[0]
+    cosang = (np.trace(pose[:3, :3].T @ G[:3, :3]) - 1) / 2
+    assert np.degrees(np.arccos(np.clip(cosang, -1, 1))) < 12.0
+
+
+def test_v_equals_sum_of_pair_counts(pkg, ctx):
+    spec = pkg.synthetic.config_plain(seed=61, n_model=500, n_plane=1500, n_box=400)
+    model, scene = _mk(pkg, ctx, spec)
+    model.ppf_lookup(scene)
+    pc = model.pair_vote_counts(scene)
+    assert model.stats["n_votes"] == int(pc.sum())
+    assert model.stats["n_matched_pairs"] == int(np.count_nonzero(pc))
+    codes, counts = model.get_votes()
+    # reference order: count descending, then code ascending
+    assert np.all(np.diff(counts.astype(np.int64)) <= 0)
+    same = counts[1:] == counts[:-1]
+    assert np.all(codes[1:][same] > codes[:-1][same])
+
+
+def test_no_votes_and_edge_sizes(pkg, ctx):
+    spec = pkg.synthetic.config_plain(seed=71, n_model=200, n_plane=100, n_box=50)
+    m, d = spec.models[0], spec.d_dists[0]
+    model = pkg.Model(m, d, 0.3, context=ctx)
+    far = (m.points + np.float32(100.0), m.normals)
+    scene = pkg.Scene(far, d, 1, context=ctx)
+    pose = model.ppf_lookup(scene, raise_on_no_votes=False)
+    # a translated copy of the model still matches (features are translation invariant)
+    assert model.stats["n_votes"] > 0
+    one = pkg.Scene((m.points[:1], m.normals[:1]), d, 1, context=ctx)
+    with pytest.raises(pkg.PPFError):
+        model.ppf_lookup(one)
+    two = pkg.Model((m.points[:2], m.normals[:2]), d, 0.3, context=ctx)
+    assert two.hash_array()["map"].size == 4
+    with pytest.raises(pkg.PPFError):
+        pkg.Model((m.points[:1], m.normals[:1]), d, 0.3, context=ctx)
+    with pytest.raises(pkg.PPFError):
+        pkg.Model(m, -1.0, 0.3, context=ctx)
+    # threshold >= 1 keeps nothing
+    strict = pkg.Model(m, d, 1.0, context=ctx)
+    sc = pkg.Scene(spec.scene, d, 5, context=ctx)
+    with pytest.raises(pkg.PPFError):
+        strict.ppf_lookup(sc)
+    assert strict.stats["n_kept"] == 0 and strict.stats["max_vote_count"] > 0
+    del pose
+
+
+def test_duplicate_points_take_exact_bins(pkg, ctx, ref_gpu):
+    """Coincident points give zero-length frame vectors; their votes must be
+    binned by the exact path and still match the reference."""
+    spec = pkg.synthetic.config_plain(seed=81, n_model=200, n_plane=200, n_box=100)
+    m = spec.models[0]
+    pts = np.concatenate([m.points, m.points[:20]])
+    nrm = np.concatenate([m.normals, m.normals[:20]])
+    s = spec.scene
+    sp = np.concatenate([s.points, s.points[:30]])
+    sn = np.concatenate([s.normals, s.normals[:30]])
+    d = spec.d_dists[0]
+    model = pkg.Model((pts, nrm), d, 0.3, context=ctx)
+    scene = pkg.Scene((sp, sn), d, 5, context=ctx)
+    codes, counts = model.all_votes(scene)
+    R = ref_gpu.lookup((pts, nrm), (sp, sn), d, 5, 0.3, all_votes=True)
+    assert np.array_equal(codes, R["all_codes"]) and np.array_equal(counts, R["all_counts"])
+
+
+def test_registration_api_matches_lookup(pkg, ctx):
+    spec = pkg.synthetic.config_plain(seed=91, n_model=300, n_plane=400, n_box=200)
+    m, s, d = spec.models[0], spec.scene, spec.d_dists[0]
+    poses, stats = pkg.ppf_registration([s, s], [m], [d], 5, 0.3, return_stats=True)
+    model = pkg.Model(m, d, 0.3, context=ctx)
+    pose = model.ppf_lookup(pkg.Scene(s, d, 5, context=ctx))
+    assert _same(poses[0][0], pose) and _same(poses[1][0], pose)
+    assert stats[0][0]["n_votes"] == model.stats["n_votes"]
+
+
+def test_device_pointer_inputs(pkg, ctx):
+    import torch
+
+    spec = pkg.synthetic.config_plain(seed=101, n_model=250, n_plane=300, n_box=100)
+    m, s, d = spec.models[0], spec.scene, spec.d_dists[0]
+    host = pkg.Model(m, d, 0.3, context=ctx).ppf_lookup(pkg.Scene(s, d, 5, context=ctx))
+    tm = (torch.from_numpy(m.points).cuda(), torch.from_numpy(m.normals).cuda())
+    ts = (torch.from_numpy(s.points).cuda(), torch.from_numpy(s.normals).cuda())
+    torch.cuda.synchronize()
+    dev = pkg.Model(tm, d, 0.3, context=ctx).ppf_lookup(pkg.Scene(ts, d, 5, context=ctx))
+    assert _same(host, dev)
+
+
+def test_cpu_clustering_mode(pkg, ctx, oracle):
+    spec = pkg.synthetic.config_plain(seed=111, n_model=300, n_plane=400, n_box=200)
+    m, s, d = spec.models[0], spec.scene, spec.d_dists[0]
+    model = pkg.Model(m, d, 0.3, cpu_clustering=True, context=ctx)
+    pose = model.ppf_lookup(pkg.Scene(s, d, 5, context=ctx))
+    T = model.getTransformations()
+    _, counts = model.get_votes()
+    out, _ = oracle.cluster_poses(T, counts, d, 2 * np.float32(np.pi) / 30)
+    assert np.allclose(pose, out[0], atol=1e-5)
