@@ -357,6 +357,10 @@ class RefGPU:
         self._err(rc, "rh_lookup")
         U = int(res.n_kept)
         nu = int(res.n_unique)
+        if all_votes and nu > acap:
+            # more unique vote cells than the buffer holds: run again with room for all
+            return self.lookup(model, scene, d_dist, ref_df, thr, use_l1_norm, use_averaged_clusters, weights,
+                               all_votes, pair_counts, cap=max(cap, nu))
         out = {
             "status": rc,
             "n_votes": int(res.n_votes),

@@ -14,9 +14,17 @@ namespace ppf {
 // Angle bins per model reference point in the vote accumulator (alpha bins
 // 0..30; bin 30 is only reached at alpha == pi exactly).
 constexpr int kBins = 31;
-// Vote kernel launch shape.
-constexpr int kVoteThreads = 512;
+#define PPF_N_ANGLE_CELLS 31
+// Vote kernel launch shape: one 1024-thread block per SM.
+constexpr int kVoteThreads = 1024;
 constexpr int kVoteWarps = kVoteThreads / 32;
+// Shared memory of the vote block besides its accumulator: per scene pair of
+// a tile its sub-run start and length, angle word, frame vector (y, z) and
+// segment offset (+1 entry).
+constexpr int kVoteQueueBytes = kVoteThreads * (4 + 4 + 4 + 8) + (kVoteThreads + 4) * 4;
+// Accumulator words of a chunk: one 32-bit counter per (m_r, alpha bin) cell
+// (the reference counts votes in unsigned int too, include/impl/util.hpp:30-52).
+inline size_t vote_acc_words(uint32_t chunk) { return ((size_t)chunk * kBins + 3) & ~size_t(3); }
 // Angle quantum on the host (include/kernel.h:16 evaluated in float).
 #define PPF_D_ANGLE_HOST ((2.0f * 3.141592654f) / float(30))
 
@@ -47,7 +55,9 @@ struct ModelTables {
   size_t P = 0;
   DevBuf keys;           // uint32 sorted keys
   DevBuf pairs;          // uint32 pair index r*n + i (the hash array's data map)
-  DevBuf entries;        // uint32 (m_r << 16) | 16-bit angle of u
+  DevBuf entries;        // uint32 ((m_r mod chunk) * 31) << 16 | 16-bit angle of u,
+                         // vote order: by key, then m_r, then a hash of the pair
+  DevBuf epairs;         // uint32 pair index of each entry (vote order)
   // runs
   size_t K = 0;
   DevBuf uniq, first, count;  // uint32 each
@@ -81,6 +91,8 @@ struct LookupState {
   DevBuf adj;         // uint32 U*27
   DevBuf scores;      // float U
   DevBuf cells_sorted, cells_map, cells_uniq, cells_first, cells_count;
+  DevBuf cells3;      // int4 U: integer cell of each pose
+  DevBuf qs, tws, adjrun, item_off;  // cell-major clustering tables
   DevBuf cand_codes, cand_counts;  // vote-pass candidates
   DevBuf tmp64, tmp32a, tmp32b, perm;
   DevBuf best;        // float[16] pose + int idx

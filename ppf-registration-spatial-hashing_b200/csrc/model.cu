@@ -55,24 +55,42 @@ __global__ void pair_keys_kernel(const float4* __restrict__ pts, const float4* _
   }
 }
 
-// Vote entry of each sorted pair: (m_r << 16) | angle16(u), u = the pair's
-// second point in the frame of the first.  A pair whose u is (numerically)
-// zero cannot be binned from angles; its run is flagged for exact binning.
-__global__ void entries_kernel(const uint32_t* __restrict__ pairs, size_t P, uint32_t n,
-                               const float4* __restrict__ pts, const float4* __restrict__ r1,
+// Vote order of the run entries: by key, then m_r, then a hash of the pair
+// index.  Grouping a run by m_r lets the vote pass split it into m_r chunks;
+// the hash scatters the pairs of one m_r over angles, so that neighbouring
+// lanes of a warp rarely count into the same (m_r, bin) cell even when the
+// cloud's points come in scan order.
+__global__ void order_words_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ pairs,
+                                   size_t P, uint32_t n, unsigned long long* __restrict__ words) {
+  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < P;
+       j += (size_t)gridDim.x * blockDim.x) {
+    uint32_t pr = pairs[j];
+    uint32_t mr = pr / n;
+    words[j] = ((unsigned long long)keys[j] << 32) | (mr << 16) | ((pr * 0x9E3779B1u) >> 16);
+  }
+}
+
+// Vote entry of each pair in vote order: ((m_r mod chunk) * 31) << 16 |
+// angle16(u), u = the pair's second point in the frame of the first: the high
+// half is the pair's accumulator row inside its m_r chunk, so the vote kernel
+// forms a cell index with one add.  A pair whose u is
+// (numerically) zero cannot be binned from angles; its run is flagged for
+// exact binning.
+__global__ void entries_kernel(const uint32_t* __restrict__ epairs, size_t P, uint32_t n,
+                               uint32_t chunk, const float4* __restrict__ pts, const float4* __restrict__ r1,
                                const float4* __restrict__ r2, const uint32_t* __restrict__ first,
                                size_t K, uint32_t* __restrict__ entries,
                                uint8_t* __restrict__ run_flags) {
   for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < P;
        j += (size_t)gridDim.x * blockDim.x) {
-    uint32_t pr = pairs[j];
+    uint32_t pr = epairs[j];
     uint32_t mr = pr / n, mi = pr - mr * n;
     FrameYZ f;
     f.r1 = r1[mr];
     f.r2 = r2[mr];
     float4 q4 = pts[mi];
     float2 u = frame_point_yz(f, make_float3(q4.x, q4.y, q4.z));
-    entries[j] = (mr << 16) | angle16(u);
+    entries[j] = (((mr % chunk) * (uint32_t)PPF_N_ANGLE_CELLS) << 16) | angle16(u);
     if (fabsf(u.x) + fabsf(u.y) < 1e-12f || !isfinite(u.x) || !isfinite(u.y)) {
       // run of position j: last run start <= j
       size_t lo = 0, hi = K;
@@ -109,8 +127,9 @@ __global__ void ht_build_kernel(const uint32_t* __restrict__ uniq, size_t K, uin
 }
 
 // split[r*(C+1) + c] = first position of run r whose m_r >= c*chunk
-// (entries of a run are in pair-index order, so m_r is non-decreasing).
-__global__ void split_kernel(const uint32_t* __restrict__ entries, const uint32_t* __restrict__ first,
+// (entries of a run are in m_r order).
+__global__ void split_kernel(const uint32_t* __restrict__ epairs, uint32_t n,
+                             const uint32_t* __restrict__ first,
                              const uint32_t* __restrict__ count, size_t K, uint32_t chunk,
                              uint32_t n_chunks, uint32_t* __restrict__ split) {
   for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < K;
@@ -123,7 +142,7 @@ __global__ void split_kernel(const uint32_t* __restrict__ entries, const uint32_
       uint32_t lo = b, hi = e;  // first position with m_r >= bound
       while (lo < hi) {
         uint32_t mid = lo + ((hi - lo) >> 1);
-        if ((entries[mid] >> 16) < bound) lo = mid + 1;
+        if (epairs[mid] / n < bound) lo = mid + 1;
         else hi = mid;
       }
       out[c] = lo;
@@ -224,15 +243,39 @@ void build_model(Context& ctx, ModelTables& t, const float* xyz, const float* nx
   PPF_CUDA(cudaMemcpyAsync(t.first.ptr, first.ptr, t.K * 4, cudaMemcpyDeviceToDevice, st));
   PPF_CUDA(cudaMemcpyAsync(t.count.ptr, count.ptr, t.K * 4, cudaMemcpyDeviceToDevice, st));
 
-  // vote entries
+  // m_r chunks sized to the vote kernel's shared-memory accumulator
+  uint32_t max_chunk = 64;
+  // (a chunk's accumulator row offsets, (m_r mod chunk) * 31, fit 16 bits)
+  while (vote_acc_words(max_chunk + 1) * 4 + kVoteQueueBytes <= (size_t)ctx.vote_smem_limit &&
+         max_chunk * (uint32_t)kBins < 65536u - kBins)
+    ++max_chunk;
+  t.n_chunks = (t.n + max_chunk - 1) / max_chunk;
+  t.chunk = (t.n + t.n_chunks - 1) / t.n_chunks;
+
+  // vote entries in vote order; epairs keeps each entry's pair index
   t.entries.reserve(t.P * sizeof(uint32_t));
+  t.epairs.reserve(t.P * sizeof(uint32_t));
   t.run_flags.reserve(t.K);
   PPF_CUDA(cudaMemsetAsync(t.run_flags.ptr, 0, t.K, st));
-  entries_kernel<<<grid_for(t.P, 256), 256, 0, st>>>(
-      t.pairs.as<uint32_t>(), t.P, t.n, t.pts.as<float4>(), t.frame_r1.as<float4>(),
-      t.frame_r2.as<float4>(), t.first.as<uint32_t>(), t.K, t.entries.as<uint32_t>(),
-      t.run_flags.as<uint8_t>());
-  PPF_CUDA(cudaGetLastError());
+  {
+    DevBuf words;
+    words.reserve(t.P * sizeof(unsigned long long));
+    order_words_kernel<<<grid_for(t.P, 256), 256, 0, st>>>(t.keys.as<uint32_t>(), t.pairs.as<uint32_t>(),
+                                                            t.P, t.n, words.as<unsigned long long>());
+    PPF_CUDA(cudaMemcpyAsync(t.epairs.ptr, t.pairs.ptr, t.P * 4, cudaMemcpyDeviceToDevice, st));
+    PPF_CUDA(cudaGetLastError());
+    size_t l1 = ctx.sort64.launches();
+    ctx.sort64.sort(words.as<unsigned long long>(), t.epairs.as<uint32_t>(), false, t.P, 0, 64, st,
+                    ctx.flags.as<uint32_t>());
+    ctx.launches += ctx.sort64.launches() - l1;
+    entries_kernel<<<grid_for(t.P, 256), 256, 0, st>>>(
+        t.epairs.as<uint32_t>(), t.P, t.n, t.chunk, t.pts.as<float4>(), t.frame_r1.as<float4>(),
+        t.frame_r2.as<float4>(), t.first.as<uint32_t>(), t.K, t.entries.as<uint32_t>(),
+        t.run_flags.as<uint8_t>());
+    PPF_CUDA(cudaGetLastError());
+    ctx.launches += 2;
+    PPF_CUDA(cudaStreamSynchronize(st));  // words is freed on scope exit
+  }
 
   // key -> run table, load factor <= 0.5
   uint32_t cap = 1024;
@@ -246,14 +289,8 @@ void build_model(Context& ctx, ModelTables& t, const float* xyz, const float* nx
                                                        t.ht_runs.as<uint32_t>());
   PPF_CUDA(cudaGetLastError());
 
-  // m_r chunks sized to the vote kernel's shared-memory accumulator
-  const int reserve_bytes = 16 * 1024;
-  uint32_t max_chunk = (uint32_t)((ctx.vote_smem_limit - reserve_bytes) / (kBins * 4));
-  if (max_chunk < 64) max_chunk = 64;
-  t.n_chunks = (t.n + max_chunk - 1) / max_chunk;
-  t.chunk = (t.n + t.n_chunks - 1) / t.n_chunks;
   t.split.reserve(t.K * (t.n_chunks + 1) * sizeof(uint32_t));
-  split_kernel<<<grid_for(t.K, 256), 256, 0, st>>>(t.entries.as<uint32_t>(), t.first.as<uint32_t>(),
+  split_kernel<<<grid_for(t.K, 256), 256, 0, st>>>(t.epairs.as<uint32_t>(), t.n, t.first.as<uint32_t>(),
                                                     t.count.as<uint32_t>(), t.K, t.chunk,
                                                     t.n_chunks, t.split.as<uint32_t>());
   PPF_CUDA(cudaGetLastError());

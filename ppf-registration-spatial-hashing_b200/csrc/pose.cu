@@ -72,6 +72,7 @@ struct PoseArgs {
   float* weighted;
   uint32_t* cell_keys;
   uint32_t* adj;
+  int4* cells3;
 };
 
 // trans_calc_kernel2 + vote_weight_kernel + mat2transquat_kernel +
@@ -110,6 +111,7 @@ __global__ void poses_kernel(PoseArgs a) {
     a.weighted[i] = a.m_w[mr] * a.counts[i];
     int3 c = trans_cell(t, a.d_dist);
     a.cell_keys[i] = cell_key(c.x, c.y, c.z);
+    a.cells3[i] = make_int4(c.x, c.y, c.z, 0);
     uint32_t* adj = a.adj + 27 * i;
     int idx = 0;
     for (int di = -1; di < 2; ++di)
@@ -182,6 +184,146 @@ __global__ void cluster_kernel(ClusterArgs a) {
     a.trans[3 * i] = to.x;
     a.trans[3 * i + 1] = to.y;
     a.trans[3 * i + 2] = to.z;
+  }
+}
+
+// ---- cell-major clustering ------------------------------------------------
+// The same scores as cluster_kernel, computed per (cell run, tile of 256
+// target poses): the poses of each neighbour cell run are streamed through
+// shared memory once per tile and tested by every target of the tile.  Each
+// target still visits its neighbours in the reference's order (neighbour
+// b = 0..26, then run order), so sums and running averages round the same.
+
+constexpr int kClusterTile = 256;
+
+__global__ void gather_sorted_kernel(const uint32_t* __restrict__ map, size_t U,
+                                     const float* __restrict__ quats, const float* __restrict__ trans0,
+                                     const float* __restrict__ weighted, float4* __restrict__ qs,
+                                     float4* __restrict__ tws) {
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < U;
+       p += (size_t)gridDim.x * blockDim.x) {
+    uint32_t o = map[p];
+    qs[p] = make_float4(quats[4 * o], quats[4 * o + 1], quats[4 * o + 2], quats[4 * o + 3]);
+    tws[p] = make_float4(trans0[3 * o], trans0[3 * o + 1], trans0[3 * o + 2], weighted[o]);
+  }
+}
+
+// Per cell run: its 27 neighbour runs (-1: none / the centre), the number of
+// target tiles, and whether all its poses share one int3 cell (two cells with
+// one hash would need per-pose neighbour lists).
+__global__ void run_adjacency_kernel(const uint32_t* __restrict__ first, const uint32_t* __restrict__ count,
+                                     size_t Kc, const uint32_t* __restrict__ map,
+                                     const int4* __restrict__ cells3, const uint32_t* __restrict__ uniq,
+                                     int* __restrict__ adjrun, uint32_t* __restrict__ tiles,
+                                     uint32_t* __restrict__ mixed) {
+  for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < Kc;
+       r += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t f = first[r], n = count[r];
+    const int4 c0 = cells3[map[f]];
+    for (uint32_t e = 1; e < n; ++e) {
+      int4 c = cells3[map[f + e]];
+      if (c.x != c0.x || c.y != c0.y || c.z != c0.z) {
+        atomicOr(mixed, 1u);
+        break;
+      }
+    }
+    int b = 0;
+    for (int di = -1; di < 2; ++di)
+      for (int dj = -1; dj < 2; ++dj)
+        for (int dk = -1; dk < 2; ++dk, ++b) {
+          int run = -1;
+          if (!(di == 0 && dj == 0 && dk == 0)) {
+            uint32_t key = cell_key(c0.x + di, c0.y + dj, c0.z + dk);
+            size_t lo = 0, hi = Kc;
+            while (lo < hi) {
+              size_t mid = (lo + hi) >> 1;
+              if (uniq[mid] < key) lo = mid + 1;
+              else hi = mid;
+            }
+            if (key != 0u && lo < Kc && uniq[lo] == key) run = (int)lo;
+          }
+          adjrun[r * 27 + b] = run;
+        }
+    tiles[r] = (n + kClusterTile - 1) / kClusterTile;
+  }
+}
+
+struct TiledArgs {
+  const uint32_t* first;
+  const uint32_t* count;
+  const uint32_t* map;
+  const int* adjrun;
+  const uint32_t* item_off;  // exclusive scan of tiles per run
+  size_t Kc;
+  uint32_t n_items;
+  const float4* qs;
+  const float4* tws;
+  float d_dist;
+  int use_l1, use_avg;
+  float* scores;
+  float* trans;
+};
+
+__global__ void __launch_bounds__(kClusterTile) cluster_tiled_kernel(TiledArgs a) {
+  __shared__ float4 sq[kClusterTile], stw[kClusterTile];
+  const float rot_sq = PPF_ROT_THRESH * PPF_ROT_THRESH;
+  for (uint32_t item = blockIdx.x; item < a.n_items; item += gridDim.x) {
+    size_t lo = 0, hi = a.Kc;  // run r with item_off[r] <= item < item_off[r + 1]
+    while (hi - lo > 1) {
+      size_t mid = (lo + hi) >> 1;
+      if (a.item_off[mid] <= item) lo = mid;
+      else hi = mid;
+    }
+    const size_t r = lo;
+    const uint32_t p = a.first[r] + (item - a.item_off[r]) * kClusterTile + threadIdx.x;
+    const bool valid = p < a.first[r] + a.count[r];
+    float4 q = make_float4(0, 0, 0, 0), tw = make_float4(0, 0, 0, 0);
+    if (valid) {
+      q = a.qs[p];
+      tw = a.tws[p];
+    }
+    const float3 t = make_float3(tw.x, tw.y, tw.z);
+    float c = 1;
+    float3 to = t;
+    for (int b = 0; b < 27; ++b) {
+      const int nr = a.adjrun[r * 27 + b];
+      if (nr < 0) continue;
+      const uint32_t f = a.first[nr], n = a.count[nr];
+      for (uint32_t s0 = 0; s0 < n; s0 += kClusterTile) {
+        __syncthreads();
+        if (s0 + threadIdx.x < n) {
+          sq[threadIdx.x] = a.qs[f + s0 + threadIdx.x];
+          stw[threadIdx.x] = a.tws[f + s0 + threadIdx.x];
+        }
+        __syncthreads();
+        if (!valid) continue;
+        const uint32_t m = min((uint32_t)kClusterTile, n - s0);
+        for (uint32_t jj = 0; jj < m; ++jj) {
+          const float qd = fabsf(8 * (1 - dot4(q, sq[jj])));
+          if (qd < rot_sq) {
+            const float4 sj = stw[jj];
+            const float3 tj = make_float3(sj.x, sj.y, sj.z);
+            if (!a.use_l1) {
+              float nd = norm3(v3_sub(t, tj));
+              if (!(nd < a.d_dist)) continue;
+            }
+            if (a.use_avg) {
+              to = v3_scale(c, to);
+              to = v3_add(to, v3_scale(sj.w, tj));
+              to = v3_scale(1 / (c + sj.w), to);
+            }
+            c += sj.w;
+          }
+        }
+      }
+    }
+    if (valid) {
+      const uint32_t o = a.map[p];
+      a.scores[o] = c;
+      a.trans[3 * o] = to.x;
+      a.trans[3 * o + 1] = to.y;
+      a.trans[3 * o + 2] = to.z;
+    }
   }
 }
 
@@ -308,6 +450,7 @@ void compute_poses(Context& ctx, const Model& m, const SceneData& s, LookupState
   a.weighted = grow<float>(st.weighted, U);
   a.cell_keys = grow<uint32_t>(st.cell_keys, U);
   a.adj = grow<uint32_t>(st.adj, U * 27);
+  a.cells3 = grow<int4>(st.cells3, U);
   grow<float>(st.trans, U * 3);
   grow<float>(st.scores, U);
   if (U <= 1) {
@@ -365,7 +508,43 @@ size_t cluster_poses_gpu(Context& ctx, const Model& m, LookupState& st, float* b
   a.use_avg = m.use_averaged_clusters;
   a.scores = st.scores.as<float>();
   a.trans = st.trans.as<float>();
-  cluster_kernel<<<grid_for(U, 128), 128, 0, stream>>>(a);
+  // cell-major tiled scores; per-pose neighbour lists only if two different
+  // cells share a hash inside one run
+  float4* qs = grow<float4>(st.qs, U);
+  float4* tws = grow<float4>(st.tws, U);
+  int* adjrun = grow<int>(st.adjrun, Kc * 27);
+  uint32_t* item_off = grow<uint32_t>(st.item_off, Kc + 1);
+  PPF_CUDA(cudaMemsetAsync(ctx.counters.ptr, 0, 8, stream));
+  uint32_t* mixed = ctx.counters.as<uint32_t>();
+  gather_sorted_kernel<<<grid_for(U, 256), 256, 0, stream>>>(map, U, a.quats, a.trans0, a.weighted, qs, tws);
+  run_adjacency_kernel<<<grid_for(Kc, 128), 128, 0, stream>>>(fi, ct, Kc, map, st.cells3.as<int4>(), uq,
+                                                              adjrun, item_off, mixed);
+  exclusive_scan_small(item_off, Kc, mixed + 1, stream);
+  uint32_t hc[2];
+  PPF_CUDA(cudaMemcpyAsync(hc, mixed, 8, cudaMemcpyDeviceToHost, stream));
+  PPF_CUDA(cudaStreamSynchronize(stream));
+  ctx.launches += 3;
+  if (hc[0]) {
+    cluster_kernel<<<grid_for(U, 128), 128, 0, stream>>>(a);
+  } else {
+    TiledArgs ta;
+    ta.first = fi;
+    ta.count = ct;
+    ta.map = map;
+    ta.adjrun = adjrun;
+    ta.item_off = item_off;
+    ta.Kc = Kc;
+    ta.n_items = hc[1];
+    ta.qs = qs;
+    ta.tws = tws;
+    ta.d_dist = m.t.d_dist;
+    ta.use_l1 = m.use_l1_norm;
+    ta.use_avg = m.use_averaged_clusters;
+    ta.scores = a.scores;
+    ta.trans = a.trans;
+    const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>(hc[1], (size_t)sm_count() * 8));
+    cluster_tiled_kernel<<<grid, kClusterTile, 0, stream>>>(ta);
+  }
   argmax_pose_kernel<<<1, 1024, 0, stream>>>(a.scores, U, st.transforms.as<float>(), a.trans, best);
   PPF_CUDA(cudaGetLastError());
   ctx.launches += 2;

@@ -289,6 +289,11 @@ void RadixSorter<K>::sort(K* keys, uint32_t* vals, bool vals_iota, size_t n, int
 template class RadixSorter<uint32_t>;
 template class RadixSorter<unsigned long long>;
 
+void exclusive_scan_small(uint32_t* v, size_t n, uint32_t* total_dev, cudaStream_t st) {
+  runs_scan_tiles<<<1, kRunThreads, 0, st>>>(v, n, total_dev);
+  PPF_CUDA(cudaGetLastError());
+}
+
 size_t build_runs(const uint32_t* sorted_keys, size_t n, uint32_t* uniq, uint32_t* first,
                   uint32_t* count, DevBuf& scratch, cudaStream_t st, size_t* launches) {
   if (n == 0) return 0;

@@ -38,4 +38,8 @@ extern template class RadixSorter<unsigned long long>;
 size_t build_runs(const uint32_t* sorted_keys, size_t n, uint32_t* uniq, uint32_t* first,
                   uint32_t* count, DevBuf& scratch, cudaStream_t st, size_t* launches);
 
+// In-place exclusive scan of n uint32 by one block (for per-run tables of at
+// most a few million entries); *total_dev receives the sum.
+void exclusive_scan_small(uint32_t* v, size_t n, uint32_t* total_dev, cudaStream_t st);
+
 }  // namespace ppf

@@ -3,29 +3,32 @@
 // scene pair features or individual votes.
 //
 // One work item = (scene reference point s_r, chunk of model reference points).
-// A persistent block takes items from an atomic counter.  For its s_r it walks
-// all scene points in tiles of 512: each thread computes one pair feature, its
-// FNV key, and looks the key up in the model's key -> run table; matched pairs
-// are queued in shared memory with their sub-run for this chunk.  The block
-// then spreads the queued votes evenly over its warps (consecutive lanes read
-// consecutive run entries) and counts each vote into a shared-memory
-// accumulator of (m_r, alpha bin) cells.  When the item is done, the block
-// folds its largest count into a global running maximum and emits every cell
-// whose count exceeds threshold x running maximum: a superset of the cells
-// the final threshold (threshold x global maximum) keeps.
+// A persistent block (1024 threads, one per SM) takes items from an atomic
+// counter.  For its s_r it walks all scene points in tiles of 1024: each
+// thread computes one pair feature, its FNV key, and looks the key up in the
+// model's key -> run table.  Every matched pair's sub-run (the run entries
+// whose m_r falls in this chunk) is cut into segments of at most kSeg entries;
+// warps take segments from a shared counter and stream their entries with
+// consecutive lanes on consecutive entries, counting each vote into a
+// shared-memory accumulator of 32-bit (m_r, alpha bin) counters.  When an
+// item is done, the block folds its largest count into a global running
+// maximum and emits every cell whose count exceeds threshold x running
+// maximum: a superset of the cells the final threshold (threshold x global
+// maximum) keeps.
 #include "engine.h"
 #include "ppf_math.cuh"
 
 namespace ppf {
 namespace {
 
-constexpr int kUnroll = 8;
-constexpr int kUnit = 32 * kUnroll;
+constexpr uint32_t kSeg = 1024;   // entries per segment
+constexpr int kUnroll = 8;        // independent entry loads per lane
+constexpr uint32_t kNoRun = 0xffffffffu;
 
 struct VoteArgs {
   // model
   const uint32_t* entries;
-  const uint32_t* pairs;
+  const uint32_t* epairs;
   const uint32_t* split;
   const uint32_t* run_count;
   const uint8_t* run_flags;
@@ -61,14 +64,13 @@ __device__ __forceinline__ uint32_t ht_lookup(const uint32_t* __restrict__ keys,
   for (uint32_t probe = 0; probe <= mask; ++probe) {
     uint32_t k = __ldg(keys + s);
     if (k == key) return __ldg(runs + s);
-    if (k == 0u) return 0xffffffffu;
+    if (k == 0u) return kNoRun;
     s = (s + 1) & mask;
   }
-  return 0xffffffffu;
+  return kNoRun;
 }
 
-__device__ __forceinline__ uint32_t block_excl_scan512(uint32_t v, uint32_t* s_warp,
-                                                       uint32_t* total) {
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* s_warp, uint32_t* total) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t x = v;
 #pragma unroll
@@ -94,21 +96,34 @@ __device__ __forceinline__ uint32_t block_excl_scan512(uint32_t v, uint32_t* s_w
   return r;
 }
 
+// Exact bin of one vote: the reference's own arithmetic for it.
+__device__ __forceinline__ uint32_t exact_bin(const VoteArgs& a, uint32_t pos, uint32_t mr,
+                                              float2 v) {
+  const uint32_t mi = __ldg(a.epairs + pos) - mr * a.n_m;
+  FrameYZ fm;
+  fm.r1 = __ldg(a.m_r1 + mr);
+  fm.r2 = __ldg(a.m_r2 + mr);
+  float4 q4 = __ldg(a.m_pts + mi);
+  float2 u = frame_point_yz(fm, make_float3(q4.x, q4.y, q4.z));
+  return alpha_bin_exact(u, v);
+}
+
 __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
   extern __shared__ __align__(16) uint32_t smem[];
-  const uint32_t cells = a.chunk * kBins;
-  uint32_t* acc = smem;
-  uint32_t* q_off = acc + ((cells + 3u) & ~3u);  // kVoteThreads + 1
-  uint32_t* q_lo = q_off + kVoteThreads + 4;
-  uint32_t* q_beta = q_lo + kVoteThreads;
-  float2* q_v = reinterpret_cast<float2*>(q_beta + kVoteThreads);
+  uint32_t* q_lo = smem;                        // [kVoteThreads]
+  uint32_t* q_len = q_lo + kVoteThreads;        // [kVoteThreads]
+  uint32_t* q_beta = q_len + kVoteThreads;      // [kVoteThreads]
+  float2* q_v = reinterpret_cast<float2*>(q_beta + kVoteThreads);       // [kVoteThreads]
+  uint32_t* q_seg = reinterpret_cast<uint32_t*>(q_v + kVoteThreads);    // [kVoteThreads + 4]
+  uint32_t* acc = q_seg + kVoteThreads + 4;
 
-  __shared__ uint32_t s_item, s_total, s_max;
+  __shared__ uint32_t s_item, s_next, s_max;
   __shared__ uint32_t s_warp[kVoteWarps];
   __shared__ float4 s_fr[2];  // scene frame rows 1, 2
   __shared__ float4 s_pr, s_nr;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t cells = a.chunk * kBins;
   unsigned long long my_votes = 0, my_matched = 0, my_exact = 0;
 
   for (;;) {
@@ -119,7 +134,7 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
     const uint32_t c = item % a.n_chunks;
     const uint32_t ref = (uint32_t)(((unsigned long long)(item / a.n_chunks) * a.perm_mul) % a.n_ref);
     const uint32_t sr = ref * a.ref_df;
-    const uint32_t mr_base = c * a.chunk;
+    const uint32_t mr_lo = c * a.chunk;
     if (tid == 0) {
       float4 p = a.s_pts[sr], q = a.s_nrm[sr];
       FrameYZ f = frame_yz(make_float3(p.x, p.y, p.z), make_float3(q.x, q.y, q.z));
@@ -148,7 +163,7 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
         uint32_t key = feature_key(f);
         if (key != 0u) {
           uint32_t run = ht_lookup(a.ht_keys, a.ht_runs, a.ht_mask, key);
-          if (run != 0xffffffffu) {
+          if (run != kNoRun) {
             const uint32_t* sp = a.split + (size_t)run * (a.n_chunks + 1);
             lo = __ldg(sp + c);
             len = __ldg(sp + c + 1) - lo;
@@ -164,75 +179,89 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
           }
         }
       }
-      uint32_t total;
-      uint32_t off = block_excl_scan512(len, s_warp, &total);
-      q_off[tid] = off;
+      uint32_t n_seg_total;
+      uint32_t seg0 = block_excl_scan((len + kSeg - 1) / kSeg, s_warp, &n_seg_total);
       q_lo[tid] = lo;
+      q_len[tid] = len;
       q_beta[tid] = beta;
       q_v[tid] = v;
-      if (tid == 0) q_off[kVoteThreads] = total;
+      q_seg[tid] = seg0;
+      if (tid == 0) {
+        q_seg[kVoteThreads] = n_seg_total;
+        s_next = kVoteWarps;
+      }
       __syncthreads();
 
-      // ---- spread the tile's votes over the warps
-      for (uint32_t ustart = (uint32_t)warp * kUnit; ustart < total; ustart += kVoteWarps * kUnit) {
-        uint32_t plo = 0, phi = kVoteThreads;
+      // ---- warps take segments; lanes stream consecutive entries
+      uint32_t s = warp;
+      while (s < n_seg_total) {
+        uint32_t plo = 0, phi = kVoteThreads;  // pair p with q_seg[p] <= s < q_seg[p+1]
         while (phi - plo > 1) {
           uint32_t mid = (plo + phi) >> 1;
-          if (q_off[mid] <= ustart) plo = mid;
+          if (q_seg[mid] <= s) plo = mid;
           else phi = mid;
         }
-        uint32_t p = plo;
-        uint32_t nxt = q_off[p + 1];
-        uint32_t pbase = q_lo[p] - q_off[p];
-        uint32_t pbeta = q_beta[p];
-        uint32_t pos[kUnroll], bs[kUnroll], pk[kUnroll], ent[kUnroll];
-#pragma unroll
-        for (int k = 0; k < kUnroll; ++k) {
-          uint32_t vi = ustart + lane + 32u * k;
-          pos[k] = 0xffffffffu;
-          if (vi < total) {
-            if (vi >= nxt) {
-              do {
-                ++p;
-                nxt = q_off[p + 1];
-              } while (vi >= nxt);
-              pbase = q_lo[p] - q_off[p];
-              pbeta = q_beta[p];
-            }
-            pos[k] = pbase + vi;
-            bs[k] = pbeta;
-            pk[k] = p;
-          }
-        }
-#pragma unroll
-        for (int k = 0; k < kUnroll; ++k)
-          if (pos[k] != 0xffffffffu) ent[k] = __ldg(a.entries + pos[k]);
-#pragma unroll
-        for (int k = 0; k < kUnroll; ++k) {
-          if (pos[k] == 0xffffffffu) continue;
-          const uint32_t mr = ent[k] >> 16;
-          int bin = (bs[k] & 0x10000u) ? -1 : alpha_bin_fast(ent[k] & 0xffffu, bs[k] & 0xffffu);
-          if (bin < 0) {
-            // exact path: the reference's own arithmetic for this vote
-            const uint32_t pr_idx = __ldg(a.pairs + pos[k]);
-            const uint32_t mi = pr_idx - mr * a.n_m;
-            FrameYZ fm;
-            fm.r1 = __ldg(a.m_r1 + mr);
-            fm.r2 = __ldg(a.m_r2 + mr);
-            float4 q4 = __ldg(a.m_pts + mi);
-            float2 u = frame_point_yz(fm, make_float3(q4.x, q4.y, q4.z));
-            bin = (int)alpha_bin_exact(u, q_v[pk[k]]);
+        const uint32_t p = plo;
+        const uint32_t start = q_lo[p] + (s - q_seg[p]) * kSeg;
+        const uint32_t end = min(q_lo[p] + q_len[p], start + kSeg);
+        const uint32_t bw = q_beta[p];
+        const uint32_t bsp = bw + 32768u;  // bits above 16 shift out below
+        const float2 vv = q_v[p];
+        // Each entry holds its accumulator row (m_r - mr_lo) * 31 in the high
+        // half and the model angle beta_m in the low half.  With y = (beta_s +
+        // 2^15 - beta_m) << 16, i.e. alpha + pi in 2^-32 turns, the bin is the
+        // high word of y * 30 and the low word is the position inside the bin.
+        const uint32_t bsh = bsp << 16;
+        constexpr uint32_t m_lo = (PPF_BIN_MARGIN_UNITS * PPF_N_ANGLE) << 16;
+        constexpr uint32_t m_span = (65536u - 2 * PPF_BIN_MARGIN_UNITS * PPF_N_ANGLE) << 16;
+        const uint32_t* ep = a.entries + start + lane;
+        const uint32_t n_here = end - start;
+        if (bw & 0x10000u) {
+          // degenerate frame vector or run: every vote takes the exact path
+          for (uint32_t k = lane; k < n_here; k += 32) {
+            const uint32_t row = __ldg(a.entries + start + k) >> 16;
+            atomicAdd(&acc[row + exact_bin(a, start + k, mr_lo + row / kBins, vv)], 1u);
             ++my_exact;
           }
-          atomicAdd(&acc[(mr - mr_base) * kBins + (uint32_t)bin], 1u);
+        } else {
+          const uint32_t nfull = n_here / (32 * kUnroll);
+          for (uint32_t it = 0; it < nfull; ++it, ep += 32 * kUnroll) {
+            uint32_t e[kUnroll];
+#pragma unroll
+            for (int u = 0; u < kUnroll; ++u) e[u] = __ldg(ep + 32 * u);
+#pragma unroll
+            for (int u = 0; u < kUnroll; ++u) {
+              const uint32_t y = bsh - (e[u] << 16);
+              uint32_t cell = (e[u] >> 16) + __umulhi(y, (uint32_t)PPF_N_ANGLE);
+              if (y * (uint32_t)PPF_N_ANGLE - m_lo > m_span) {  // near a bin edge
+                const uint32_t row = e[u] >> 16;
+                cell = row + exact_bin(a, (uint32_t)(ep + 32 * u - a.entries), mr_lo + row / kBins, vv);
+                ++my_exact;
+              }
+              atomicAdd(&acc[cell], 1u);
+            }
+          }
+          for (uint32_t k = nfull * 32 * kUnroll + lane; k < n_here; k += 32) {
+            const uint32_t e = __ldg(a.entries + start + k);
+            const uint32_t y = bsh - (e << 16);
+            uint32_t cell = (e >> 16) + __umulhi(y, (uint32_t)PPF_N_ANGLE);
+            if (y * (uint32_t)PPF_N_ANGLE - m_lo > m_span) {
+              const uint32_t row = e >> 16;
+              cell = row + exact_bin(a, start + k, mr_lo + row / kBins, vv);
+              ++my_exact;
+            }
+            atomicAdd(&acc[cell], 1u);
+          }
         }
+        if (lane == 0) s = atomicAdd(&s_next, 1u);
+        s = __shfl_sync(0xffffffffu, s, 0);
       }
       __syncthreads();
     }
 
-    // ---- fold the item's maximum into the running maximum, emit cells
+    // ---- running maximum, emission
     uint32_t lmax = 0;
-    for (uint32_t i = tid; i < cells; i += kVoteThreads) lmax = max(lmax, acc[i]);
+    for (uint32_t w = tid; w < cells; w += kVoteThreads) lmax = max(lmax, acc[w]);
 #pragma unroll
     for (int o = 16; o; o >>= 1) lmax = max(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
     if (lane == 0) s_warp[warp] = lmax;
@@ -247,7 +276,7 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
     const float floor_v = a.floor >= 0.f ? a.floor : a.thr * (float)s_max;
     for (uint32_t b0 = 0; b0 < cells; b0 += kVoteThreads) {
       const uint32_t cell = b0 + tid;
-      uint32_t cnt = cell < cells ? acc[cell] : 0u;
+      const uint32_t cnt = cell < cells ? acc[cell] : 0u;
       bool keep = cnt != 0u && (a.emit_all || (float)cnt > floor_v);
       uint32_t ballot = __ballot_sync(0xffffffffu, keep);
       if (!ballot) continue;
@@ -255,11 +284,11 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
       if (lane == 0) slot0 = atomicAdd(a.n_cand, (uint32_t)__popc(ballot));
       slot0 = __shfl_sync(0xffffffffu, slot0, 0);
       if (keep) {
-        uint32_t slot = slot0 + __popc(ballot & ((1u << lane) - 1u));
-        if (slot < a.cand_cap) {
-          uint32_t mr = mr_base + cell / kBins, bin = cell % kBins;
-          a.cand_code[slot] = ((unsigned long long)sr << 32) | ((unsigned long long)mr << 6) | bin;
-          a.cand_count[slot] = cnt;
+        uint32_t sl = slot0 + __popc(ballot & ((1u << lane) - 1u));
+        if (sl < a.cand_cap) {
+          uint32_t mr = mr_lo + cell / kBins, bin = cell % kBins;
+          a.cand_code[sl] = ((unsigned long long)sr << 32) | ((unsigned long long)mr << 6) | bin;
+          a.cand_count[sl] = cnt;
         } else {
           atomicOr(a.flags, (uint32_t)kFlagCandidateOverflow);
         }
@@ -298,7 +327,7 @@ __global__ void pair_vote_counts_kernel(VoteArgs a, unsigned long long* __restri
         uint32_t key = feature_key(f);
         if (key) {
           uint32_t run = ht_lookup(a.ht_keys, a.ht_runs, a.ht_mask, key);
-          if (run != 0xffffffffu) cnt = a.run_count[run];
+          if (run != kNoRun) cnt = a.run_count[run];
         }
       }
       row[i] = cnt;
@@ -319,7 +348,7 @@ VoteArgs make_args(const Model& m, const SceneData& s) {
   const ModelTables& t = m.t;
   VoteArgs a{};
   a.entries = t.entries.as<uint32_t>();
-  a.pairs = t.pairs.as<uint32_t>();
+  a.epairs = t.epairs.as<uint32_t>();
   a.split = t.split.as<uint32_t>();
   a.run_count = t.count.as<uint32_t>();
   a.run_flags = t.run_flags.as<uint8_t>();
@@ -358,7 +387,7 @@ VoteResult run_votes(Context& ctx, const Model& m, const SceneData& s, LookupSta
   a.floor = floor;
   a.n_items = a.n_ref * a.n_chunks;
   if (s.n < 2 || a.n_items == 0) return r;
-  // counters: [0] work, [1] max, [2] n_cand, [3] pad, then 3 x u64 stats
+  // counters: [0] work, [1] max, [2] n_cand, [3] pad, [4..9] 3 x u64 stats
   ctx.counters.reserve(64);
   PPF_CUDA(cudaMemsetAsync(ctx.counters.ptr, 0, 64, stream));
   PPF_CUDA(cudaMemsetAsync(ctx.flags.ptr, 0, sizeof(uint32_t), stream));
@@ -374,21 +403,16 @@ VoteResult run_votes(Context& ctx, const Model& m, const SceneData& s, LookupSta
   a.cand_count = st.cand_counts.as<uint32_t>();
   a.cand_cap = (uint32_t)cand_cap;
 
-  const uint32_t cells = a.chunk * kBins;
-  size_t smem = (size_t)((cells + 3u) & ~3u) * 4 + (kVoteThreads + 4) * 4 + kVoteThreads * 4 * 2 +
-                kVoteThreads * 8;
+  const size_t smem = kVoteQueueBytes + vote_acc_words(a.chunk) * 4;
   PPF_REQUIRE((int)smem <= ctx.vote_smem_limit, PPF_ERR_INTERNAL, "vote accumulator too large");
   PPF_CUDA(cudaFuncSetAttribute(vote_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  unsigned grid = (unsigned)std::min<size_t>(a.n_items, (size_t)sm_count());
   PPF_CUDA(cudaEventRecord(ctx.ev[0], stream));
-  vote_kernel<<<grid, kVoteThreads, smem, stream>>>(a);
+  vote_kernel<<<(unsigned)std::min<size_t>(a.n_items, (size_t)sm_count()), kVoteThreads, smem, stream>>>(a);
   PPF_CUDA(cudaGetLastError());
-  PPF_CUDA(cudaEventRecord(ctx.ev[1], stream));
   ctx.launches++;
+  PPF_CUDA(cudaEventRecord(ctx.ev[1], stream));
   uint32_t h[16];
   PPF_CUDA(cudaMemcpyAsync(h, ctx.counters.ptr, 64, cudaMemcpyDeviceToHost, stream));
-  uint32_t flags = 0;
-  PPF_CUDA(cudaMemcpyAsync(&flags, ctx.flags.ptr, 4, cudaMemcpyDeviceToHost, stream));
   PPF_CUDA(cudaStreamSynchronize(stream));
   PPF_CUDA(cudaEventElapsedTime(&r.vote_ms, ctx.ev[0], ctx.ev[1]));
   r.max_count = h[1];

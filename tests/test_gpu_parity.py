@@ -113,13 +113,27 @@ def test_lookup_modes(pkg, ctx, ref_gpu, mode):
     assert np.array_equal(codes, R["codes"]) and np.array_equal(counts, R["counts"])
     t, q, s = model.get_cluster_state()
     if mode == "avg":
-        # the reference reads neighbour translations while other threads
-        # overwrite them; scores are unaffected, translations agree to 1e-5 diam
-        assert _same(s, R["scores"])
-        tol = 1e-5 * spec.diameters[0]
-        assert np.max(np.abs(t - R["trans"])) <= tol
-        assert np.max(np.abs(pose[:3, 3] - R["pose"][:3, 3])) <= tol
-        assert _same(pose[:3, :3], R["pose"][:3, :3])
+        # With averaged clusters the reference updates translations in place
+        # while other threads read them for their distance tests and averages
+        # (src/cuda/kernel.cu:741-758): its scores then depend on thread timing
+        # (on this case about half differ from its own non-averaged scores and
+        # about 1% from a rerun).  This engine reads the translations from
+        # before clustering, so its averaged-mode scores equal the
+        # non-averaged scores, which match the reference bit for bit.
+        assert _same(model.getTransformations(), R["transforms"])
+        assert _same(q, R["quats"])
+        plain = pkg.Model(spec.models[0], spec.d_dists[0], spec.vote_count_threshold, context=ctx)
+        plain.ppf_lookup(scene)
+        Rp = ref_gpu.lookup((spec.models[0].points, spec.models[0].normals),
+                            (spec.scene.points, spec.scene.normals), spec.d_dists[0], spec.ref_point_df,
+                            spec.vote_count_threshold)
+        assert _same(s, plain.get_cluster_state()[2])
+        assert _same(s, Rp["scores"])
+        # an average of translations within d_dist of the pose stays within d_dist
+        d = spec.d_dists[0]
+        t0 = plain.get_cluster_state()[0]
+        assert np.max(np.linalg.norm(t - t0, axis=1)) < d
+        assert np.max(np.abs(t - R["trans"])) < d
     else:
         # float sums of weights may round differently in another order;
         # integer weights (the reference's case) are exact
@@ -251,3 +265,25 @@ def test_cpu_clustering_mode(pkg, ctx, oracle):
     _, counts = model.get_votes()
     out, _ = oracle.cluster_poses(T, counts, d, 2 * np.float32(np.pi) / 30)
     assert np.allclose(pose, out[0], atol=1e-5)
+
+
+def test_large_cell_count(pkg, ctx):
+    """70,000 identical scene pairs vote into one (s_r, m_r, alpha) cell: the
+    shared-memory counter and the emitted count must be exact past 16 bits."""
+    n_copies = 70000
+    p0 = np.array([[0.0, 0.0, 0.0]], np.float32)
+    n0 = np.array([[0.0, 0.0, 1.0]], np.float32)
+    p1 = np.array([[0.05, 0.01, 0.02]], np.float32)
+    n1 = np.array([[0.3, 0.2, 0.9]], np.float32)
+    n1 /= np.linalg.norm(n1)
+    model = (np.concatenate([p0, p1]), np.concatenate([n0, n1]))
+    scene = (np.concatenate([p0, np.repeat(p1, n_copies, 0)]), np.concatenate([n0, np.repeat(n1, n_copies, 0)]))
+    d = 0.01
+    M = pkg.Model(model, d, 0.3, context=ctx)
+    S = pkg.Scene(scene, d, n_copies + 1, context=ctx)  # point 0 is the only reference point
+    codes, counts = M.all_votes(S)
+    assert int(counts.max()) == n_copies
+    assert int(counts.sum()) == n_copies
+    M.ppf_lookup(S, raise_on_no_votes=False)
+    assert M.stats["max_vote_count"] == n_copies
+    assert M.stats["n_votes"] == n_copies
