@@ -55,6 +55,7 @@ typedef struct ppf_stats {
   float vote_ms;             /* device time of the vote pass */
   float total_ms;            /* device time of the whole lookup */
   uint32_t gpu_launches;     /* kernels launched by the lookup */
+  uint32_t n_redo_items;     /* vote items emitted again after the candidate buffer grew */
 } ppf_stats;
 
 /* Error text of the last failing call on this thread ("" if none). */

@@ -37,6 +37,7 @@ class ppf_stats(C.Structure):
         ("vote_ms", C.c_float),
         ("total_ms", C.c_float),
         ("gpu_launches", C.c_uint32),
+        ("n_redo_items", C.c_uint32),
     ]
 
     def as_dict(self):

@@ -2,6 +2,7 @@
 // catches engine errors and returns a status; the message is kept per thread.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -13,6 +14,16 @@
 namespace ppf {
 
 Context::~Context() {
+  // device blocks go back to the pool on this stream, so free them first
+  flags.release();
+  counters.release();
+  scratch.release();
+  cand_codes.release();
+  cand_counts.release();
+  redo_items.release();
+  sort32.release();
+  sort64.release();
+  if (stream) cudaStreamSynchronize(stream);
   for (auto& e : ev)
     if (e) cudaEventDestroy(e);
   if (stream) cudaStreamDestroy(stream);
@@ -46,8 +57,6 @@ void copy_out(void* dst, const void* src_dev, size_t bytes, cudaStream_t st) {
   PPF_CUDA(cudaMemcpyAsync(dst, src_dev, bytes, cudaMemcpyDefault, st));
 }
 
-constexpr size_t kInitialCandidates = size_t(1) << 22;
-
 struct LookupOut {
   ppf_status status = PPF_OK;
   float pose[16] = {0};
@@ -61,30 +70,20 @@ LookupOut lookup(Model& m, const SceneData& s) {
   LookupOut out;
   const size_t launches0 = ctx.launches;
   PPF_CUDA(cudaEventRecord(ctx.ev[2], ctx.stream));
-  size_t cap = std::max(kInitialCandidates, st.cand_codes.bytes / sizeof(unsigned long long));
-  VoteResult vr = run_votes(ctx, m, s, st, false, -1.f, cap);
+  VoteResult vr = run_votes(ctx, m, s, false, -1.f);
   st.U = 0;
   out.stats.n_votes = vr.n_votes;
   out.stats.n_matched_pairs = vr.n_matched;
   out.stats.n_exact_bins = vr.n_exact;
   out.stats.max_vote_count = vr.max_count;
   out.stats.vote_ms = vr.vote_ms;
+  out.stats.n_redo_items = vr.n_redo;
   if (vr.max_count == 0) {
     out.status = PPF_ERR_NO_VOTES;
     return out;
   }
   const float min_votecount = m.vote_count_threshold * (float)vr.max_count;
   out.stats.min_votecount = min_votecount;
-  if (vr.n_cand > cap) {
-    // Emission buffer overflowed: run again with the final threshold, which
-    // emits exactly the kept cells (at most n_cand of them).
-    cap = vr.n_cand;
-    VoteResult vr2 = run_votes(ctx, m, s, st, false, min_votecount, cap);
-    PPF_REQUIRE(vr2.n_cand <= cap && vr2.max_count == vr.max_count, PPF_ERR_INTERNAL,
-                "vote pass is not reproducible");
-    out.stats.vote_ms += vr2.vote_ms;
-    vr.n_cand = vr2.n_cand;
-  }
   out.stats.n_candidates = vr.n_cand;
   const size_t U = select_votes(ctx, m, s, st, vr.n_cand, min_votecount);
   out.stats.n_kept = U;
@@ -116,7 +115,8 @@ LookupOut lookup(Model& m, const SceneData& s) {
   PPF_CUDA(cudaEventRecord(ctx.ev[3], ctx.stream));
   PPF_CUDA(cudaStreamSynchronize(ctx.stream));
   uint32_t flags = 0;
-  PPF_CUDA(cudaMemcpy(&flags, ctx.flags.ptr, 4, cudaMemcpyDeviceToHost));
+  PPF_CUDA(cudaMemcpyAsync(&flags, ctx.flags.ptr, 4, cudaMemcpyDeviceToHost, ctx.stream));
+  PPF_CUDA(cudaStreamSynchronize(ctx.stream));
   PPF_REQUIRE(!(flags & kFlagSpinTimeout), PPF_ERR_TIMEOUT, "radix sort look-back timed out");
   PPF_CUDA(cudaEventElapsedTime(&out.stats.total_ms, ctx.ev[2], ctx.ev[3]));
   out.stats.gpu_launches = (uint32_t)(ctx.launches - launches0);
@@ -136,12 +136,25 @@ void init_context(Context& c, int device) {
   PPF_CUDA(cudaSetDevice(c.device));
   PPF_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
   for (auto& e : c.ev) PPF_CUDA(cudaEventCreate(&e));
+  // keep freed blocks in the device's stream-ordered pool for reuse
+  cudaMemPool_t pool;
+  PPF_CUDA(cudaDeviceGetDefaultMemPool(&pool, c.device));
+  uint64_t keep = UINT64_MAX;
+  PPF_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  StreamScope scope(c.stream);
   c.flags.reserve(256);
   c.counters.reserve(256);
-  PPF_CUDA(cudaMemset(c.flags.ptr, 0, 256));
+  PPF_CUDA(cudaMemsetAsync(c.flags.ptr, 0, 256, c.stream));
+  PPF_CUDA(cudaStreamSynchronize(c.stream));
   int optin = 0;
   PPF_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device));
   c.vote_smem_limit = optin - 2048;  // static shared memory of the vote kernel
+  if (const char* e = std::getenv("PPF_B200_CHECKS")) c.checks = e[0] == '1';
+  // test hook: a small initial candidate buffer exercises its growth path
+  if (const char* e = std::getenv("PPF_B200_CANDIDATE_CAP")) {
+    long long v = std::atoll(e);
+    if (v > 0) c.cand_cap = (size_t)v;
+  }
 }
 
 }  // namespace
@@ -195,6 +208,7 @@ ppf_status ppf_model_create(ppf_context_t ctx, const float* xyz, const float* nx
     PPF_REQUIRE(std::isfinite(vote_count_threshold) && vote_count_threshold >= 0.f,
                 PPF_ERR_INVALID_ARGUMENT, "vote_count_threshold must be finite and >= 0");
     PPF_CUDA(cudaSetDevice(ctx->c.device));
+    StreamScope scope(ctx->c.stream);
     std::unique_ptr<ppf_model_s> m(new ppf_model_s());
     m->m.ctx = &ctx->c;
     m->m.vote_count_threshold = vote_count_threshold;
@@ -212,6 +226,7 @@ ppf_status ppf_model_set_point_vote_weights(ppf_model_t m, const float* w, uint6
     PPF_REQUIRE(m && w, PPF_ERR_INVALID_ARGUMENT, "null model or weights");
     PPF_REQUIRE(n == m->m.t.n, PPF_ERR_INVALID_ARGUMENT, "one weight per model point required");
     PPF_CUDA(cudaSetDevice(m->m.ctx->device));
+    StreamScope scope(m->m.ctx->stream);
     PPF_CUDA(cudaMemcpyAsync(m->m.t.weights.ptr, w, n * sizeof(float), cudaMemcpyDefault,
                              m->m.ctx->stream));
     PPF_CUDA(cudaStreamSynchronize(m->m.ctx->stream));
@@ -223,6 +238,7 @@ ppf_status ppf_model_destroy(ppf_model_t m) {
   return guarded([&]() {
     if (m) {
       cudaSetDevice(m->m.ctx->device);
+      StreamScope scope(m->m.ctx->stream);
       cudaStreamSynchronize(m->m.ctx->stream);
       delete m;
     }
@@ -242,6 +258,7 @@ ppf_status ppf_scene_create(ppf_context_t ctx, const float* xyz, const float* nx
     PPF_REQUIRE(d_dist > 0.f && std::isfinite(d_dist), PPF_ERR_INVALID_ARGUMENT,
                 "d_dist must be a positive finite number");
     PPF_CUDA(cudaSetDevice(ctx->c.device));
+    StreamScope scope(ctx->c.stream);
     std::unique_ptr<ppf_scene_s> s(new ppf_scene_s());
     s->ctx = &ctx->c;
     s->s.n = (uint32_t)n;
@@ -258,6 +275,7 @@ ppf_status ppf_scene_destroy(ppf_scene_t s) {
   return guarded([&]() {
     if (s) {
       cudaSetDevice(s->ctx->device);
+      StreamScope scope(s->ctx->stream);
       cudaStreamSynchronize(s->ctx->stream);
       delete s;
     }
@@ -270,6 +288,7 @@ ppf_status ppf_model_lookup(ppf_model_t m, ppf_scene_t s, float* pose_out, ppf_s
     PPF_REQUIRE(m && s && pose_out, PPF_ERR_INVALID_ARGUMENT, "null model, scene or pose");
     PPF_REQUIRE(m->m.ctx == s->ctx, PPF_ERR_INVALID_ARGUMENT, "model and scene on different contexts");
     PPF_CUDA(cudaSetDevice(m->m.ctx->device));
+    StreamScope scope(m->m.ctx->stream);
     LookupOut r = lookup(m->m, s->s);
     PPF_CUDA(cudaMemcpy(pose_out, r.pose, sizeof(r.pose), cudaMemcpyDefault));
     if (stats) *stats = r.stats;
@@ -301,6 +320,7 @@ ppf_status ppf_registration(ppf_context_t ctx, uint64_t n_scenes, const float* c
       c = own.get();
     }
     PPF_CUDA(cudaSetDevice(c->c.device));
+    StreamScope scope(c->c.stream);
     std::vector<float> host_poses(n_scenes * n_models * 16, 0.f);
     ppf_status worst = PPF_OK;
     for (uint64_t j = 0; j < n_models; ++j) {
@@ -402,6 +422,7 @@ ppf_status ppf_pair_keys(ppf_context_t ctx, const float* xyz, const float* nxyz,
     PPF_REQUIRE(n <= 65535, PPF_ERR_INVALID_ARGUMENT, "pair keys limited to 65535 points");
     Context& c = ctx->c;
     PPF_CUDA(cudaSetDevice(c.device));
+    StreamScope scope(c.stream);
     DevBuf p, q, k;
     upload_points(c, xyz, n, p);
     upload_points(c, nxyz, n, q);
@@ -423,11 +444,9 @@ ppf_status ppf_model_all_votes(ppf_model_t m, ppf_scene_t s, uint64_t* codes, ui
     PPF_REQUIRE(m && s && n, PPF_ERR_INVALID_ARGUMENT, "null model, scene or count");
     Context& c = *m->m.ctx;
     PPF_CUDA(cudaSetDevice(c.device));
+    StreamScope scope(c.stream);
     LookupState& st = m->m.last;
-    size_t want = (size_t)((s->s.n + s->s.ref_df - 1) / s->s.ref_df) * m->m.t.n * kBins;
-    size_t capc = std::min<size_t>(std::max<size_t>(want, 1), size_t(1) << 28);
-    VoteResult vr = run_votes(c, m->m, s->s, st, true, -1.f, capc);
-    PPF_REQUIRE(vr.n_cand <= capc, PPF_ERR_OUT_OF_MEMORY, "too many vote cells for a dump");
+    VoteResult vr = run_votes(c, m->m, s->s, true, -1.f);
     sort_by_code(c, st, vr.n_cand);
     st.U = 0;
     *n = vr.n_cand;
@@ -445,6 +464,7 @@ ppf_status ppf_model_pair_vote_counts(ppf_model_t m, ppf_scene_t s, uint64_t* co
     PPF_REQUIRE(m && s && counts, PPF_ERR_INVALID_ARGUMENT, "null model, scene or counts");
     Context& c = *m->m.ctx;
     PPF_CUDA(cudaSetDevice(c.device));
+    StreamScope scope(c.stream);
     const size_t nn = (size_t)s->s.n * s->s.n;
     DevBuf tmp;
     uint64_t* dst = counts;

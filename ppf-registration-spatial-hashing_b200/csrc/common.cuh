@@ -33,20 +33,52 @@ struct Error : public std::runtime_error {
     if (!(cond)) throw ::ppf::Error((status), (msg)); \
   } while (0)
 
+// The stream that device allocations of the current call are ordered on.
+// Every C-ABI entry point that allocates sets it to its context's stream
+// (StreamScope); allocations then come from the device's stream-ordered pool
+// and freed blocks are reused by later calls without a device synchronise.
+inline cudaStream_t& alloc_stream() {
+  thread_local cudaStream_t s = nullptr;
+  return s;
+}
+
+struct StreamScope {
+  cudaStream_t prev;
+  explicit StreamScope(cudaStream_t s) : prev(alloc_stream()) { alloc_stream() = s; }
+  ~StreamScope() { alloc_stream() = prev; }
+};
+
 // Owning device allocation, grown on demand, never shrunk implicitly.
 struct DevBuf {
   void* ptr = nullptr;
   size_t bytes = 0;
+  cudaStream_t stream = nullptr;  // stream the block was allocated on (freed there too)
+  bool pooled = false;
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
-  DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), bytes(o.bytes) {
+  DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), bytes(o.bytes), stream(o.stream), pooled(o.pooled) {
     o.ptr = nullptr;
     o.bytes = 0;
   }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      ptr = o.ptr;
+      bytes = o.bytes;
+      stream = o.stream;
+      pooled = o.pooled;
+      o.ptr = nullptr;
+      o.bytes = 0;
+    }
+    return *this;
+  }
   ~DevBuf() { release(); }
   void release() {
-    if (ptr) cudaFree(ptr);
+    if (ptr) {
+      if (pooled) cudaFreeAsync(ptr, stream);
+      else cudaFree(ptr);
+    }
     ptr = nullptr;
     bytes = 0;
   }
@@ -54,7 +86,10 @@ struct DevBuf {
     if (b <= bytes) return;
     release();
     size_t want = b < 256 ? 256 : b;
-    PPF_CUDA(cudaMalloc(&ptr, want));
+    stream = alloc_stream();
+    pooled = stream != nullptr;
+    if (pooled) PPF_CUDA(cudaMallocAsync(&ptr, want, stream));
+    else PPF_CUDA(cudaMalloc(&ptr, want));
     bytes = want;
   }
   template <typename T>
@@ -88,6 +123,7 @@ enum DeviceFlag : uint32_t {
   kFlagSpinTimeout = 1u << 0,
   kFlagCandidateOverflow = 1u << 1,
   kFlagBadInput = 1u << 2,
+  kFlagBadIndex = 1u << 3,
 };
 
 }  // namespace ppf

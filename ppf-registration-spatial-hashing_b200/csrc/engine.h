@@ -36,9 +36,13 @@ struct Context {
   DevBuf flags;      // uint32 device flags (kFlag*)
   DevBuf counters;   // small device counters for kernels
   DevBuf scratch;    // run-table scratch
+  // vote-pass candidate cells (code, count), kept and grown across lookups
+  DevBuf cand_codes, cand_counts, redo_items;
+  size_t cand_cap = size_t(1) << 24;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   int vote_smem_limit = 0;  // max dynamic shared memory per vote block
   size_t launches = 0;      // kernels launched (running total)
+  bool checks = false;      // self-checking kernels (PPF_B200_CHECKS=1)
   ~Context();
 };
 
@@ -93,7 +97,6 @@ struct LookupState {
   DevBuf cells_sorted, cells_map, cells_uniq, cells_first, cells_count;
   DevBuf cells3;      // int4 U: integer cell of each pose
   DevBuf qs, tws, adjrun, item_off;  // cell-major clustering tables
-  DevBuf cand_codes, cand_counts;  // vote-pass candidates
   DevBuf tmp64, tmp32a, tmp32b, perm;
   DevBuf best;        // float[16] pose + int idx
   std::vector<float> cpu_poses;
@@ -122,13 +125,13 @@ struct VoteResult {
   uint32_t max_count = 0;
   uint64_t n_votes = 0, n_matched = 0, n_exact = 0;
   uint64_t n_cand = 0;
+  uint32_t n_redo = 0;  // items emitted by a second launch after the buffer grew
   float vote_ms = 0;
 };
-// Runs the vote pass.  emit_all: emit every nonzero cell (no threshold).
-// floor >= 0 forces the emission floor (used when re-running after a
-// candidate-buffer overflow).  Candidates land in st.cand_codes/cand_counts.
-VoteResult run_votes(Context& ctx, const Model& m, const SceneData& s, LookupState& st,
-                     bool emit_all, float floor, size_t cand_cap);
+// Runs the vote pass.  emit_all: emit every nonzero cell (no threshold);
+// floor >= 0 forces the emission floor.  Candidates land in
+// ctx.cand_codes / ctx.cand_counts.
+VoteResult run_votes(Context& ctx, const Model& m, const SceneData& s, bool emit_all, float floor);
 void pair_vote_counts(Context& ctx, const Model& m, const SceneData& s, uint64_t* out_dev);
 
 // ---- poses and clustering (pose.cu)

@@ -151,6 +151,53 @@ __global__ void split_kernel(const uint32_t* __restrict__ epairs, uint32_t n,
   }
 }
 
+// Self-checking build (PPF_B200_CHECKS=1): verifies the invariants the vote
+// pass relies on and records the first violation as (site, index) in bad[].
+__global__ void validate_tables_kernel(const uint32_t* __restrict__ keys, size_t P,
+                                       const uint32_t* __restrict__ uniq, const uint32_t* __restrict__ first,
+                                       const uint32_t* __restrict__ count, size_t K,
+                                       const uint32_t* __restrict__ epairs,
+                                       const uint32_t* __restrict__ entries, uint32_t n, uint32_t chunk,
+                                       uint32_t n_chunks, const uint32_t* __restrict__ split,
+                                       unsigned long long* bad, uint32_t* flags) {
+  auto report = [&](unsigned long long site, unsigned long long idx) {
+    if (atomicCAS(&bad[0], 0ull, site) == 0ull) bad[1] = idx;
+    atomicOr(flags, (uint32_t)kFlagBadIndex);
+  };
+  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < P;
+       j += (size_t)gridDim.x * blockDim.x) {
+    if (j + 1 < P && keys[j] > keys[j + 1]) report(101, j);
+    const uint32_t pr = epairs[j];
+    if (pr >= (uint32_t)(n * n)) report(102, j);
+    const uint32_t mr = pr / n;
+    if ((entries[j] >> 16) != (mr % chunk) * (uint32_t)kBins) report(103, j);
+  }
+  for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < K;
+       r += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t b = first[r], e = b + count[r];
+    if (e > P || count[r] == 0) report(104, r);
+    if (r + 1 < K && (uniq[r] >= uniq[r + 1] || first[r + 1] != e)) report(105, r);
+    if (keys[b] != uniq[r]) report(106, r);
+    for (uint32_t j = b + 1; j < e && j < P; ++j)
+      if (epairs[j] / n < epairs[j - 1] / n) {
+        report(107, r);
+        break;
+      }
+    const uint32_t* sp = split + r * (n_chunks + 1);
+    if (sp[0] != b || sp[n_chunks] != e) report(108, r);
+    for (uint32_t c = 0; c < n_chunks; ++c) {
+      if (sp[c] > sp[c + 1]) report(109, r);
+      for (uint32_t j = sp[c]; j < sp[c + 1] && j < P; ++j) {
+        const uint32_t mr = epairs[j] / n;
+        if (mr < c * chunk || mr >= (c + 1) * chunk) {
+          report(110, r);
+          break;
+        }
+      }
+    }
+  }
+}
+
 __global__ void fill_f32(float* p, size_t n, float v) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
@@ -182,7 +229,6 @@ void upload_points(Context& ctx, const float* xyz, size_t n, DevBuf& dst) {
   pack_points_kernel<<<grid_for(n, 256), 256, 0, ctx.stream>>>(src, n, dst.as<float4>());
   PPF_CUDA(cudaGetLastError());
   ctx.launches++;
-  PPF_CUDA(cudaStreamSynchronize(ctx.stream));  // tmp is freed on return
 }
 
 void pair_keys_device(Context& ctx, const float4* pts, const float4* nrm, uint32_t n,
@@ -274,7 +320,6 @@ void build_model(Context& ctx, ModelTables& t, const float* xyz, const float* nx
         t.run_flags.as<uint8_t>());
     PPF_CUDA(cudaGetLastError());
     ctx.launches += 2;
-    PPF_CUDA(cudaStreamSynchronize(st));  // words is freed on scope exit
   }
 
   // key -> run table, load factor <= 0.5
@@ -295,10 +340,24 @@ void build_model(Context& ctx, ModelTables& t, const float* xyz, const float* nx
                                                     t.n_chunks, t.split.as<uint32_t>());
   PPF_CUDA(cudaGetLastError());
   ctx.launches += 3;
+  unsigned long long* bad = reinterpret_cast<unsigned long long*>(ctx.flags.as<uint32_t>() + 8);
+  if (ctx.checks) {
+    PPF_CUDA(cudaMemsetAsync(bad, 0, 24, st));
+    validate_tables_kernel<<<grid_for(t.P, 256), 256, 0, st>>>(
+        t.keys.as<uint32_t>(), t.P, t.uniq.as<uint32_t>(), t.first.as<uint32_t>(),
+        t.count.as<uint32_t>(), t.K, t.epairs.as<uint32_t>(), t.entries.as<uint32_t>(), t.n, t.chunk,
+        t.n_chunks, t.split.as<uint32_t>(), bad, ctx.flags.as<uint32_t>());
+    PPF_CUDA(cudaGetLastError());
+  }
   uint32_t flags = 0;
+  unsigned long long badh[2] = {0, 0};
   PPF_CUDA(cudaMemcpyAsync(&flags, ctx.flags.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  if (ctx.checks) PPF_CUDA(cudaMemcpyAsync(badh, bad, 16, cudaMemcpyDeviceToHost, st));
   PPF_CUDA(cudaStreamSynchronize(st));
   PPF_REQUIRE(!(flags & kFlagSpinTimeout), PPF_ERR_TIMEOUT, "radix sort look-back timed out");
+  PPF_REQUIRE(!(flags & kFlagBadIndex), PPF_ERR_INTERNAL,
+              "model tables inconsistent: check " + std::to_string(badh[0]) + " at " +
+                  std::to_string(badh[1]));
 }
 
 }  // namespace ppf

@@ -390,7 +390,7 @@ size_t select_votes(Context& ctx, const Model& m, const SceneData& s, LookupStat
   uint32_t* fcount = grow<uint32_t>(st.tmp32a, n_cand + 1);
   PPF_CUDA(cudaMemsetAsync(ctx.counters.ptr, 0, 4, stream));
   filter_kernel<<<grid_for(n_cand, 256), 256, 0, stream>>>(
-      st.cand_codes.as<unsigned long long>(), st.cand_counts.as<uint32_t>(), n_cand, min_votecount,
+      ctx.cand_codes.as<unsigned long long>(), ctx.cand_counts.as<uint32_t>(), n_cand, min_votecount,
       fcode, fcount, ctx.counters.as<uint32_t>());
   PPF_CUDA(cudaGetLastError());
   ctx.launches++;
@@ -423,8 +423,8 @@ void sort_by_code(Context& ctx, LookupState& st, size_t n) {
   cudaStream_t stream = ctx.stream;
   unsigned long long* code = grow<unsigned long long>(st.codes, n);
   uint32_t* count = grow<uint32_t>(st.counts, n);
-  PPF_CUDA(cudaMemcpyAsync(code, st.cand_codes.ptr, n * 8, cudaMemcpyDeviceToDevice, stream));
-  PPF_CUDA(cudaMemcpyAsync(count, st.cand_counts.ptr, n * 4, cudaMemcpyDeviceToDevice, stream));
+  PPF_CUDA(cudaMemcpyAsync(code, ctx.cand_codes.ptr, n * 8, cudaMemcpyDeviceToDevice, stream));
+  PPF_CUDA(cudaMemcpyAsync(count, ctx.cand_counts.ptr, n * 4, cudaMemcpyDeviceToDevice, stream));
   PPF_CUDA(cudaMemsetAsync(ctx.flags.ptr, 0, 4, stream));
   size_t l0 = ctx.sort64.launches();
   ctx.sort64.sort(code, count, false, n, 0, 64, stream, ctx.flags.as<uint32_t>());

@@ -12,6 +12,15 @@ constexpr unsigned long long kAgg = 1ull << 32;  // status: tile aggregate only
 constexpr unsigned long long kInc = 2ull << 32;  // status: inclusive prefix
 constexpr int kSpinLimit = 1 << 22;
 
+// Status words of other tiles change while a tile waits on them: read them
+// with a load the compiler must repeat.
+__device__ __forceinline__ unsigned long long load_status(const unsigned long long* p) {
+  return *reinterpret_cast<const volatile unsigned long long*>(p);
+}
+__device__ __forceinline__ void store_status(unsigned long long* p, unsigned long long v) {
+  *reinterpret_cast<volatile unsigned long long*>(p) = v;
+}
+
 // Exclusive scan of one value per thread over a 256-thread block.
 __device__ __forceinline__ uint32_t block_excl_scan256(uint32_t v, uint32_t* s_warp,
                                                        uint32_t* total) {
@@ -48,10 +57,18 @@ __global__ void __launch_bounds__(kThreads) rs_histogram(const K* __restrict__ k
   __shared__ uint32_t sh[8][kRadix];
   for (int i = threadIdx.x; i < 8 * kRadix; i += blockDim.x) sh[i / kRadix][i % kRadix] = 0;
   __syncthreads();
+  // one shared atomic per distinct digit of a warp: sorted or skewed keys
+  // (long runs of equal digits) would otherwise serialise on one counter
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
     K k = keys[i];
-    for (int p = 0; p < passes; ++p) atomicAdd(&sh[p][(uint32_t)(k >> (begin_bit + 8 * p)) & 0xffu], 1u);
+    const uint32_t active = __activemask();
+    const int lane = threadIdx.x & 31;
+    for (int p = 0; p < passes; ++p) {
+      const uint32_t d = (uint32_t)(k >> (begin_bit + 8 * p)) & 0xffu;
+      const uint32_t peers = __match_any_sync(active, d);
+      if (lane == __ffs(peers) - 1) atomicAdd(&sh[p][d], (uint32_t)__popc(peers));
+    }
   }
   __syncthreads();
   for (int i = threadIdx.x; i < passes * kRadix; i += blockDim.x) {
@@ -120,13 +137,13 @@ __global__ void __launch_bounds__(kThreads) rs_onesweep(
   unsigned long long* my = status + (size_t)tile * kRadix + tid;
   uint32_t excl = 0;
   if (tile == 0) {
-    __stcg(my, kInc | (unsigned long long)tile_cnt);
+    store_status(my, kInc | (unsigned long long)tile_cnt);
   } else {
-    __stcg(my, kAgg | (unsigned long long)tile_cnt);
+    store_status(my, kAgg | (unsigned long long)tile_cnt);
     long long t = (long long)tile - 1;
     while (t >= 0) {
       const unsigned long long* p = status + (size_t)t * kRadix + tid;
-      unsigned long long v = __ldcg(p);
+      unsigned long long v = load_status(p);
       int spins = 0;
       while ((v >> 32) == 0) {
         if (++spins > kSpinLimit) {
@@ -135,13 +152,13 @@ __global__ void __launch_bounds__(kThreads) rs_onesweep(
           break;
         }
         __nanosleep(32);
-        v = __ldcg(p);
+        v = load_status(p);
       }
       excl += (uint32_t)v;
       if ((v >> 32) == 2) break;
       --t;
     }
-    __stcg(my, kInc | (unsigned long long)(excl + tile_cnt));
+    store_status(my, kInc | (unsigned long long)(excl + tile_cnt));
   }
   s_global[tid] = pass_base + excl;
   __syncthreads();

@@ -23,6 +23,13 @@ class RadixSorter {
   void sort(K* keys, uint32_t* vals, bool vals_iota, size_t n, int begin_bit, int end_bit,
             cudaStream_t st, uint32_t* d_flags);
   size_t launches() const { return launches_; }
+  void release() {
+    kalt_.release();
+    valt_.release();
+    hist_.release();
+    status_.release();
+    counters_.release();
+  }
 
  private:
   DevBuf kalt_, valt_, hist_, status_, counters_;

@@ -15,6 +15,8 @@
 // maximum and emits every cell whose count exceeds threshold x running
 // maximum: a superset of the cells the final threshold (threshold x global
 // maximum) keeps.
+#include <cstring>
+
 #include "engine.h"
 #include "ppf_math.cuh"
 
@@ -54,8 +56,32 @@ struct VoteArgs {
   uint32_t* cand_count;
   uint32_t* n_cand;
   uint32_t cand_cap;
+  unsigned long long* n_needed;  // cells all items asked to emit
+  uint32_t* redo_items;          // items that did not fit the buffer
+  uint32_t* n_redo;
+  uint32_t n_items_total;        // capacity of redo_items
+  const uint32_t* item_list;     // second launch: the items to redo (else all items)
   uint32_t* flags;
+  // bounds for the self-checking build (PPF_B200_CHECKS=1)
+  size_t P, K;
+  unsigned long long* bad;  // first out-of-range access: site, value, bound
 };
+
+// Self-checking build: every index the kernel derives is compared with its
+// bound; the first violation is recorded (site, value, bound) in bad[0..2],
+// kFlagBadIndex is raised and the access is skipped.
+template <bool kCheck>
+__device__ __forceinline__ bool in_range(const VoteArgs& a, uint32_t site, unsigned long long v,
+                                         unsigned long long bound) {
+  if (!kCheck) return true;
+  if (v < bound) return true;
+  if (atomicCAS(&a.bad[0], 0ull, (unsigned long long)site) == 0ull) {
+    a.bad[1] = v;
+    a.bad[2] = bound;
+  }
+  atomicOr(a.flags, (uint32_t)kFlagBadIndex);
+  return false;
+}
 
 __device__ __forceinline__ uint32_t ht_lookup(const uint32_t* __restrict__ keys,
                                               const uint32_t* __restrict__ runs, uint32_t mask,
@@ -70,7 +96,23 @@ __device__ __forceinline__ uint32_t ht_lookup(const uint32_t* __restrict__ keys,
   return kNoRun;
 }
 
-__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* s_warp, uint32_t* total) {
+// Block barrier of the vote kernel.  Each warp is gathered (__syncwarp) and
+// its shared-memory stores are fenced before it arrives, and its loads after
+// the barrier are fenced again.  Without the fences the -O3 build of this
+// kernel was seen to let warp 0 fall one barrier phase behind the others on
+// one 60000-point scene (the other warps read the segment scan before warp 0
+// had written it); with them, and with -Xptxas -O1 or -O0, it did not.
+__device__ __forceinline__ void block_sync() {
+  __syncwarp();
+  __threadfence_block();
+  __syncthreads();
+  __threadfence_block();
+}
+
+// Exclusive block scan of one value per thread; `total` receives the sum.
+// s_warp is this call site's own 32-word scratch; the caller places a barrier
+// between two scans on the same scratch (both call sites have several).
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* s_warp, uint32_t& total) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t x = v;
 #pragma unroll
@@ -79,27 +121,31 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* s_warp
     if (lane >= o) x += y;
   }
   if (lane == 31) s_warp[warp] = x;
-  __syncthreads();
+  block_sync();
   if (warp == 0) {
-    uint32_t w = lane < kVoteWarps ? s_warp[lane] : 0u;
+    uint32_t w = s_warp[lane];
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
       if (lane >= o) w += y;
     }
-    if (lane < kVoteWarps) s_warp[lane] = w;
+    s_warp[lane] = w;
   }
-  __syncthreads();
-  uint32_t r = (warp ? s_warp[warp - 1] : 0u) + x - v;
-  if (total) *total = s_warp[kVoteWarps - 1];
-  __syncthreads();
+  block_sync();
+  const uint32_t r = (warp ? s_warp[warp - 1] : 0u) + x - v;
+  total = s_warp[kVoteWarps - 1];
   return r;
 }
 
-// Exact bin of one vote: the reference's own arithmetic for it.
-__device__ __forceinline__ uint32_t exact_bin(const VoteArgs& a, uint32_t pos, uint32_t mr,
-                                              float2 v) {
-  const uint32_t mi = __ldg(a.epairs + pos) - mr * a.n_m;
+// Exact bin of one vote: the reference's own arithmetic for it.  The model
+// pair comes from the entry's pair index, so every index is in range by
+// construction.
+template <bool kCheck>
+__device__ __forceinline__ uint32_t exact_bin(const VoteArgs& a, uint32_t pos, float2 v) {
+  if (!in_range<kCheck>(a, 20, pos, a.P)) return 0;
+  const uint32_t pr = __ldg(a.epairs + pos);
+  const uint32_t mr = pr / a.n_m, mi = pr - mr * a.n_m;
+  if (!in_range<kCheck>(a, 21, mr, a.n_m) || !in_range<kCheck>(a, 22, mi, a.n_m)) return 0;
   FrameYZ fm;
   fm.r1 = __ldg(a.m_r1 + mr);
   fm.r2 = __ldg(a.m_r2 + mr);
@@ -108,6 +154,7 @@ __device__ __forceinline__ uint32_t exact_bin(const VoteArgs& a, uint32_t pos, u
   return alpha_bin_exact(u, v);
 }
 
+template <bool kCheck>
 __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
   extern __shared__ __align__(16) uint32_t smem[];
   uint32_t* q_lo = smem;                        // [kVoteThreads]
@@ -117,39 +164,39 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
   uint32_t* q_seg = reinterpret_cast<uint32_t*>(q_v + kVoteThreads);    // [kVoteThreads + 4]
   uint32_t* acc = q_seg + kVoteThreads + 4;
 
-  __shared__ uint32_t s_item, s_next, s_max;
-  __shared__ uint32_t s_warp[kVoteWarps];
-  __shared__ float4 s_fr[2];  // scene frame rows 1, 2
-  __shared__ float4 s_pr, s_nr;
+  __shared__ uint32_t s_item, s_next, s_max, s_base;
+  __shared__ uint32_t s_scan_seg[kVoteWarps];   // scratch of the per-tile segment scan
+  __shared__ uint32_t s_scan_emit[kVoteWarps];  // scratch of the emission scan
+  __shared__ uint32_t s_wmax[kVoteWarps];       // per-warp maxima of the accumulator
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t cells = a.chunk * kBins;
   unsigned long long my_votes = 0, my_matched = 0, my_exact = 0;
 
   for (;;) {
-    if (tid == 0) s_item = atomicAdd(a.work_counter, 1u);
-    __syncthreads();
-    const uint32_t item = s_item;
-    if (item >= a.n_items) break;
+    if (warp == 0) {
+      uint32_t next = 0;
+      if (lane == 0) next = atomicAdd(a.work_counter, 1u);
+      next = __shfl_sync(0xffffffffu, next, 0);
+      if (lane == 0) s_item = next;
+    }
+    block_sync();
+    const uint32_t slot_of_item = s_item;
+    if (slot_of_item >= a.n_items) break;
+    const uint32_t item = a.item_list ? a.item_list[slot_of_item] : slot_of_item;
     const uint32_t c = item % a.n_chunks;
+    // ref < n_ref, so sr = ref * ref_df < n_s
     const uint32_t ref = (uint32_t)(((unsigned long long)(item / a.n_chunks) * a.perm_mul) % a.n_ref);
     const uint32_t sr = ref * a.ref_df;
     const uint32_t mr_lo = c * a.chunk;
-    if (tid == 0) {
-      float4 p = a.s_pts[sr], q = a.s_nrm[sr];
-      FrameYZ f = frame_yz(make_float3(p.x, p.y, p.z), make_float3(q.x, q.y, q.z));
-      s_fr[0] = f.r1;
-      s_fr[1] = f.r2;
-      s_pr = p;
-      s_nr = q;
-    }
+    // every thread derives the frame of s_r itself (a broadcast load and a
+    // few dozen flops per item), so no lane-divergent code precedes a barrier
+    const float4 p4 = a.s_pts[sr], n4 = a.s_nrm[sr];
+    const float3 pr = make_float3(p4.x, p4.y, p4.z);
+    const float3 nr = make_float3(n4.x, n4.y, n4.z);
+    const FrameYZ fs = frame_yz(pr, nr);
     for (uint32_t i = tid; i < cells; i += kVoteThreads) acc[i] = 0u;
-    __syncthreads();
-    const float3 pr = make_float3(s_pr.x, s_pr.y, s_pr.z);
-    const float3 nr = make_float3(s_nr.x, s_nr.y, s_nr.z);
-    FrameYZ fs;
-    fs.r1 = s_fr[0];
-    fs.r2 = s_fr[1];
+    block_sync();
 
     for (uint32_t base = 0; base < a.n_s; base += kVoteThreads) {
       // ---- one scene pair per thread: feature, key, lookup, sub-run
@@ -163,11 +210,12 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
         uint32_t key = feature_key(f);
         if (key != 0u) {
           uint32_t run = ht_lookup(a.ht_keys, a.ht_runs, a.ht_mask, key);
-          if (run != kNoRun) {
+          if (run != kNoRun && in_range<kCheck>(a, 2, run, a.K)) {
             const uint32_t* sp = a.split + (size_t)run * (a.n_chunks + 1);
             lo = __ldg(sp + c);
             len = __ldg(sp + c + 1) - lo;
-            if (c == 0) {
+            if (kCheck && !in_range<kCheck>(a, 3, (unsigned long long)lo + len, a.P + 1)) len = 0;
+            if (c == 0 && !a.item_list) {
               my_votes += __ldg(a.run_count + run);
               my_matched += 1;
             }
@@ -180,7 +228,7 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
         }
       }
       uint32_t n_seg_total;
-      uint32_t seg0 = block_excl_scan((len + kSeg - 1) / kSeg, s_warp, &n_seg_total);
+      const uint32_t seg0 = block_excl_scan((len + kSeg - 1) / kSeg, s_scan_seg, n_seg_total);
       q_lo[tid] = lo;
       q_len[tid] = len;
       q_beta[tid] = beta;
@@ -190,7 +238,12 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
         q_seg[kVoteThreads] = n_seg_total;
         s_next = kVoteWarps;
       }
-      __syncthreads();
+      block_sync();
+      if (kCheck) {
+        const uint32_t want = q_seg[tid] + (q_len[tid] + kSeg - 1) / kSeg;
+        if (q_seg[tid] != seg0 || q_seg[tid + 1] != want)
+          in_range<kCheck>(a, 11, ((unsigned long long)tid << 32) | q_seg[tid + 1], want);
+      }
 
       // ---- warps take segments; lanes stream consecutive entries
       uint32_t s = warp;
@@ -203,7 +256,25 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
         }
         const uint32_t p = plo;
         const uint32_t start = q_lo[p] + (s - q_seg[p]) * kSeg;
-        const uint32_t end = min(q_lo[p] + q_len[p], start + kSeg);
+        uint32_t end = min(q_lo[p] + q_len[p], start + kSeg);
+        // Always-on guard (one compare per segment of up to 1024 votes): a
+        // segment outside its sub-run or the entry array is recorded, raises
+        // kFlagBadIndex and is skipped, so the lookup fails instead of the
+        // kernel reading outside the entries.
+        if (start >= end || end > a.P) {
+          if (lane == 0) {
+            if (atomicCAS(&a.bad[3], 0ull, 1ull) == 0ull) {
+              a.bad[4] = ((unsigned long long)p << 32) | s;
+              a.bad[5] = ((unsigned long long)q_seg[p] << 32) | q_seg[p + 1];
+              a.bad[6] = ((unsigned long long)q_lo[p] << 32) | q_len[p];
+              a.bad[7] = ((unsigned long long)n_seg_total << 32) | q_seg[kVoteThreads];
+              a.bad[8] = ((unsigned long long)base << 32) | item;
+              a.bad[9] = ((unsigned long long)warp << 32) | plo;
+            }
+            atomicOr(a.flags, (uint32_t)kFlagBadIndex);
+          }
+          end = start;
+        }
         const uint32_t bw = q_beta[p];
         const uint32_t bsp = bw + 32768u;  // bits above 16 shift out below
         const float2 vv = q_v[p];
@@ -220,7 +291,8 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
           // degenerate frame vector or run: every vote takes the exact path
           for (uint32_t k = lane; k < n_here; k += 32) {
             const uint32_t row = __ldg(a.entries + start + k) >> 16;
-            atomicAdd(&acc[row + exact_bin(a, start + k, mr_lo + row / kBins, vv)], 1u);
+            const uint32_t cell = row + exact_bin<kCheck>(a, start + k, vv);
+            if (in_range<kCheck>(a, 6, cell, cells)) atomicAdd(&acc[cell], 1u);
             ++my_exact;
           }
         } else {
@@ -234,11 +306,10 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
               const uint32_t y = bsh - (e[u] << 16);
               uint32_t cell = (e[u] >> 16) + __umulhi(y, (uint32_t)PPF_N_ANGLE);
               if (y * (uint32_t)PPF_N_ANGLE - m_lo > m_span) {  // near a bin edge
-                const uint32_t row = e[u] >> 16;
-                cell = row + exact_bin(a, (uint32_t)(ep + 32 * u - a.entries), mr_lo + row / kBins, vv);
+                cell = (e[u] >> 16) + exact_bin<kCheck>(a, (uint32_t)(ep + 32 * u - a.entries), vv);
                 ++my_exact;
               }
-              atomicAdd(&acc[cell], 1u);
+              if (in_range<kCheck>(a, 7, cell, cells)) atomicAdd(&acc[cell], 1u);
             }
           }
           for (uint32_t k = nfull * 32 * kUnroll + lane; k < n_here; k += 32) {
@@ -246,55 +317,96 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
             const uint32_t y = bsh - (e << 16);
             uint32_t cell = (e >> 16) + __umulhi(y, (uint32_t)PPF_N_ANGLE);
             if (y * (uint32_t)PPF_N_ANGLE - m_lo > m_span) {
-              const uint32_t row = e >> 16;
-              cell = row + exact_bin(a, start + k, mr_lo + row / kBins, vv);
+              cell = (e >> 16) + exact_bin<kCheck>(a, start + k, vv);
               ++my_exact;
             }
-            atomicAdd(&acc[cell], 1u);
+            if (in_range<kCheck>(a, 8, cell, cells)) atomicAdd(&acc[cell], 1u);
           }
         }
         if (lane == 0) s = atomicAdd(&s_next, 1u);
         s = __shfl_sync(0xffffffffu, s, 0);
       }
-      __syncthreads();
+      if (kCheck && (q_seg[tid] != seg0 || q_len[tid] != len || q_lo[tid] != lo))
+        in_range<kCheck>(a, 12, ((unsigned long long)tid << 32) | q_seg[tid], seg0);
+      // No barrier here: the next tile writes the queue only after the two
+      // barriers of its segment scan, which every warp reaches after its
+      // last segment.
     }
+    block_sync();  // all votes of the item are counted
 
     // ---- running maximum, emission
     uint32_t lmax = 0;
     for (uint32_t w = tid; w < cells; w += kVoteThreads) lmax = max(lmax, acc[w]);
 #pragma unroll
     for (int o = 16; o; o >>= 1) lmax = max(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
-    if (lane == 0) s_warp[warp] = lmax;
-    __syncthreads();
-    if (tid == 0) {
-      uint32_t m = 0;
-      for (int w = 0; w < kVoteWarps; ++w) m = max(m, s_warp[w]);
-      uint32_t old = atomicMax(a.global_max, m);
-      s_max = max(old, m);
+    if (lane == 0) s_wmax[warp] = lmax;
+    block_sync();
+    if (warp == 0) {
+      uint32_t m = s_wmax[lane];
+#pragma unroll
+      for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+      uint32_t old = 0;
+      if (lane == 0) old = atomicMax(a.global_max, m);
+      old = __shfl_sync(0xffffffffu, old, 0);
+      if (lane == 0) s_max = max(old, m);
     }
-    __syncthreads();
+    block_sync();
     const float floor_v = a.floor >= 0.f ? a.floor : a.thr * (float)s_max;
-    for (uint32_t b0 = 0; b0 < cells; b0 += kVoteThreads) {
-      const uint32_t cell = b0 + tid;
-      const uint32_t cnt = cell < cells ? acc[cell] : 0u;
-      bool keep = cnt != 0u && (a.emit_all || (float)cnt > floor_v);
-      uint32_t ballot = __ballot_sync(0xffffffffu, keep);
-      if (!ballot) continue;
-      uint32_t slot0 = 0;
-      if (lane == 0) slot0 = atomicAdd(a.n_cand, (uint32_t)__popc(ballot));
-      slot0 = __shfl_sync(0xffffffffu, slot0, 0);
-      if (keep) {
-        uint32_t sl = slot0 + __popc(ballot & ((1u << lane) - 1u));
-        if (sl < a.cand_cap) {
-          uint32_t mr = mr_lo + cell / kBins, bin = cell % kBins;
-          a.cand_code[sl] = ((unsigned long long)sr << 32) | ((unsigned long long)mr << 6) | bin;
-          a.cand_count[sl] = cnt;
-        } else {
-          atomicOr(a.flags, (uint32_t)kFlagCandidateOverflow);
+    // All-or-nothing slot reservation for the item's cells: an item that does
+    // not fit writes nothing and is queued for a second launch after the
+    // buffer has grown, so the buffer never holds a partial item.
+    uint32_t my_n = 0;
+    for (uint32_t cell = tid; cell < cells; cell += kVoteThreads) {
+      const uint32_t cnt = acc[cell];
+      my_n += (cnt != 0u && (a.emit_all || (float)cnt > floor_v)) ? 1u : 0u;
+    }
+    uint32_t item_total;
+    const uint32_t my_off = block_excl_scan(my_n, s_scan_emit, item_total);
+    if (warp == 0) {
+      // The whole warp walks the reservation loop in lockstep (lane 0 issues
+      // the atomics, every exit condition is warp-uniform).
+      uint32_t base_slot = 0xffffffffu;
+      if (item_total) {
+        if (lane == 0) atomicAdd(a.n_needed, (unsigned long long)item_total);
+        uint32_t old = 0;
+        if (lane == 0) old = *(volatile uint32_t*)a.n_cand;
+        old = __shfl_sync(0xffffffffu, old, 0);
+        for (int tries = 0; tries < (1 << 20); ++tries) {
+          if ((unsigned long long)old + item_total > a.cand_cap) break;
+          uint32_t prev = 0;
+          if (lane == 0) prev = atomicCAS(a.n_cand, old, old + item_total);
+          prev = __shfl_sync(0xffffffffu, prev, 0);
+          if (prev == old) {
+            base_slot = old;
+            break;
+          }
+          old = prev;
+        }
+        if (base_slot == 0xffffffffu && lane == 0) {
+          const uint32_t k = atomicAdd(a.n_redo, 1u);
+          if (in_range<kCheck>(a, 9, k, a.n_items_total)) a.redo_items[k] = item;
+        }
+      }
+      if (lane == 0) s_base = base_slot;
+    }
+    block_sync();
+    const uint32_t item_base = s_base;
+    if (item_base != 0xffffffffu) {
+      uint32_t slot = item_base + my_off;
+      for (uint32_t cell = tid; cell < cells; cell += kVoteThreads) {
+        const uint32_t cnt = acc[cell];
+        if (cnt != 0u && (a.emit_all || (float)cnt > floor_v)) {
+          const uint32_t mr = mr_lo + cell / kBins, bin = cell % kBins;
+          if (in_range<kCheck>(a, 10, slot, a.cand_cap)) {
+            a.cand_code[slot] = ((unsigned long long)sr << 32) | ((unsigned long long)mr << 6) | bin;
+            a.cand_count[slot] = cnt;
+          }
+          ++slot;
         }
       }
     }
-    __syncthreads();
+    // The item-fetch barrier at the top of the loop separates these reads of
+    // the accumulator from the next item's clear.
   }
 
   // per-block statistics
@@ -355,6 +467,8 @@ VoteArgs make_args(const Model& m, const SceneData& s) {
   a.ht_keys = t.ht_keys.as<uint32_t>();
   a.ht_runs = t.ht_runs.as<uint32_t>();
   a.ht_mask = t.ht_mask;
+  a.P = t.P;
+  a.K = t.K;
   a.m_r1 = t.frame_r1.as<float4>();
   a.m_r2 = t.frame_r2.as<float4>();
   a.m_pts = t.pts.as<float4>();
@@ -378,42 +492,102 @@ VoteArgs make_args(const Model& m, const SceneData& s) {
 
 }  // namespace
 
-VoteResult run_votes(Context& ctx, const Model& m, const SceneData& s, LookupState& st,
-                     bool emit_all, float floor, size_t cand_cap) {
+VoteResult run_votes(Context& ctx, const Model& m, const SceneData& s, bool emit_all, float floor) {
   VoteResult r;
   cudaStream_t stream = ctx.stream;
   VoteArgs a = make_args(m, s);
   a.emit_all = emit_all ? 1 : 0;
   a.floor = floor;
-  a.n_items = a.n_ref * a.n_chunks;
-  if (s.n < 2 || a.n_items == 0) return r;
-  // counters: [0] work, [1] max, [2] n_cand, [3] pad, [4..9] 3 x u64 stats
+  const uint32_t n_items = a.n_ref * a.n_chunks;
+  if (s.n < 2 || n_items == 0) return r;
+  // counters: [0] work, [1] max, [2] n_cand, [3] n_redo, [4..9] 3 x u64 stats,
+  // [10..11] u64 n_needed, [12] work counter of the second launch
   ctx.counters.reserve(64);
   PPF_CUDA(cudaMemsetAsync(ctx.counters.ptr, 0, 64, stream));
-  PPF_CUDA(cudaMemsetAsync(ctx.flags.ptr, 0, sizeof(uint32_t), stream));
+  // flags word and the bad-index record at byte 32 (site, value, bound, 7 words of detail)
+  PPF_CUDA(cudaMemsetAsync(ctx.flags.ptr, 0, 32 + 80, stream));
   uint32_t* cnt = ctx.counters.as<uint32_t>();
   a.work_counter = cnt + 0;
   a.global_max = cnt + 1;
   a.n_cand = cnt + 2;
+  a.n_redo = cnt + 3;
   a.stats = reinterpret_cast<unsigned long long*>(cnt + 4);
+  a.n_needed = reinterpret_cast<unsigned long long*>(cnt + 10);
   a.flags = ctx.flags.as<uint32_t>();
-  st.cand_codes.reserve(cand_cap * sizeof(unsigned long long));
-  st.cand_counts.reserve(cand_cap * sizeof(uint32_t));
-  a.cand_code = st.cand_codes.as<unsigned long long>();
-  a.cand_count = st.cand_counts.as<uint32_t>();
-  a.cand_cap = (uint32_t)cand_cap;
+  ctx.cand_codes.reserve(ctx.cand_cap * sizeof(unsigned long long));
+  ctx.cand_counts.reserve(ctx.cand_cap * sizeof(uint32_t));
+  ctx.redo_items.reserve((size_t)n_items * sizeof(uint32_t));
+  a.cand_code = ctx.cand_codes.as<unsigned long long>();
+  a.cand_count = ctx.cand_counts.as<uint32_t>();
+  a.cand_cap = (uint32_t)std::min<size_t>(ctx.cand_cap, 0xffffffffu);
+  a.redo_items = ctx.redo_items.as<uint32_t>();
+  a.item_list = nullptr;
+  a.n_items = n_items;
+  a.n_items_total = n_items;
+  const bool check = ctx.checks;
+  a.bad = reinterpret_cast<unsigned long long*>(ctx.flags.as<uint32_t>() + 8);
+  auto kernel = check ? vote_kernel<true> : vote_kernel<false>;
 
   const size_t smem = kVoteQueueBytes + vote_acc_words(a.chunk) * 4;
   PPF_REQUIRE((int)smem <= ctx.vote_smem_limit, PPF_ERR_INTERNAL, "vote accumulator too large");
-  PPF_CUDA(cudaFuncSetAttribute(vote_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  PPF_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   PPF_CUDA(cudaEventRecord(ctx.ev[0], stream));
-  vote_kernel<<<(unsigned)std::min<size_t>(a.n_items, (size_t)sm_count()), kVoteThreads, smem, stream>>>(a);
+  kernel<<<(unsigned)std::min<size_t>(n_items, (size_t)sm_count()), kVoteThreads, smem, stream>>>(a);
   PPF_CUDA(cudaGetLastError());
   ctx.launches++;
-  PPF_CUDA(cudaEventRecord(ctx.ev[1], stream));
   uint32_t h[16];
   PPF_CUDA(cudaMemcpyAsync(h, ctx.counters.ptr, 64, cudaMemcpyDeviceToHost, stream));
   PPF_CUDA(cudaStreamSynchronize(stream));
+  if (h[3]) {
+    // Items that did not fit: grow the buffer (keeping what was emitted) to
+    // what every item asked for, then count those items again.
+    unsigned long long needed;
+    memcpy(&needed, h + 10, sizeof(needed));
+    const size_t want = std::max<size_t>(needed, 2 * ctx.cand_cap);
+    PPF_REQUIRE(want < 0xffffffffull, PPF_ERR_OUT_OF_MEMORY, "more than 2^32 vote candidates");
+    DevBuf nc, nn, items;
+    nc.reserve(want * sizeof(unsigned long long));
+    nn.reserve(want * sizeof(uint32_t));
+    items.reserve((size_t)h[3] * sizeof(uint32_t));
+    PPF_CUDA(cudaMemcpyAsync(nc.ptr, ctx.cand_codes.ptr, (size_t)h[2] * 8, cudaMemcpyDeviceToDevice, stream));
+    PPF_CUDA(cudaMemcpyAsync(nn.ptr, ctx.cand_counts.ptr, (size_t)h[2] * 4, cudaMemcpyDeviceToDevice, stream));
+    PPF_CUDA(cudaMemcpyAsync(items.ptr, ctx.redo_items.ptr, (size_t)h[3] * 4, cudaMemcpyDeviceToDevice, stream));
+    ctx.cand_codes = std::move(nc);
+    ctx.cand_counts = std::move(nn);
+    ctx.cand_cap = want;
+    a.cand_code = ctx.cand_codes.as<unsigned long long>();
+    a.cand_count = ctx.cand_counts.as<uint32_t>();
+    a.cand_cap = (uint32_t)want;
+    a.item_list = items.as<uint32_t>();
+    a.n_items = h[3];
+    a.work_counter = cnt + 12;
+    PPF_CUDA(cudaMemsetAsync(a.n_redo, 0, 4, stream));
+    kernel<<<(unsigned)std::min<size_t>(a.n_items, (size_t)sm_count()), kVoteThreads, smem, stream>>>(a);
+    PPF_CUDA(cudaGetLastError());
+    ctx.launches++;
+    r.n_redo = h[3];
+    PPF_CUDA(cudaMemcpyAsync(h, ctx.counters.ptr, 64, cudaMemcpyDeviceToHost, stream));
+    PPF_CUDA(cudaStreamSynchronize(stream));
+    PPF_REQUIRE(h[3] == 0, PPF_ERR_INTERNAL, "vote candidates still do not fit");
+  }
+  PPF_CUDA(cudaEventRecord(ctx.ev[1], stream));
+  PPF_CUDA(cudaEventSynchronize(ctx.ev[1]));
+  {
+    // flags word and bad-index record in one read
+    unsigned long long rec[14];
+    PPF_CUDA(cudaMemcpyAsync(rec, ctx.flags.ptr, sizeof(rec), cudaMemcpyDeviceToHost, stream));
+    PPF_CUDA(cudaStreamSynchronize(stream));
+    const uint32_t f = (uint32_t)(rec[0] & 0xffffffffu);
+    if (f & kFlagBadIndex) {
+      const unsigned long long* bad = rec + 4;
+      std::string detail;
+      for (int k = 3; k < 10; ++k)
+        detail += " " + std::to_string(bad[k] >> 32) + ":" + std::to_string(bad[k] & 0xffffffffu);
+      throw Error(PPF_ERR_INTERNAL, "vote kernel index out of range: site " + std::to_string(bad[0]) +
+                                        " value " + std::to_string(bad[1]) + " bound " +
+                                        std::to_string(bad[2]) + " |" + detail);
+    }
+  }
   PPF_CUDA(cudaEventElapsedTime(&r.vote_ms, ctx.ev[0], ctx.ev[1]));
   r.max_count = h[1];
   r.n_cand = h[2];

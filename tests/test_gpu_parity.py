@@ -287,3 +287,21 @@ def test_large_cell_count(pkg, ctx):
     M.ppf_lookup(S, raise_on_no_votes=False)
     assert M.stats["max_vote_count"] == n_copies
     assert M.stats["n_votes"] == n_copies
+
+
+def test_candidate_buffer_growth(pkg, ctx, monkeypatch):
+    """A candidate buffer too small for the emitted cells grows and the items
+    that did not fit are counted again: results identical to a roomy buffer."""
+    spec = pkg.synthetic.config_plain(seed=121, n_model=400, n_plane=900, n_box=300)
+    m, s, d = spec.models[0], spec.scene, spec.d_dists[0]
+    ref = pkg.Model(m, d, 0.3, context=ctx)
+    pose_ref = ref.ppf_lookup(pkg.Scene(s, d, 5, context=ctx))
+    codes_ref, counts_ref = ref.get_votes()
+    monkeypatch.setenv("PPF_B200_CANDIDATE_CAP", "64")
+    small = pkg.Context(0)
+    M = pkg.Model(m, d, 0.3, context=small)
+    pose = M.ppf_lookup(pkg.Scene(s, d, 5, context=small))
+    assert M.stats["n_redo_items"] > 0
+    codes, counts = M.get_votes()
+    assert np.array_equal(codes, codes_ref) and np.array_equal(counts, counts_ref)
+    assert _same(pose, pose_ref)
