@@ -164,6 +164,53 @@ ppf_status ppf_model_all_votes(ppf_model_t m, ppf_scene_t s, uint64_t* codes, ui
  * scene pair (r, i) matches, else 0.  counts: host or device, n_s*n_s uint64. */
 ppf_status ppf_model_pair_vote_counts(ppf_model_t m, ppf_scene_t s, uint64_t* counts);
 
+/* Allocation-free vote pass.  No counterpart in the reference: the
+ * reference allocates its vote buffers on every lookup
+ * (src/cuda/model.cu:95-171).
+ *
+ * For callers that must not allocate device memory while they run: a serving
+ * process whose device-memory budget was reserved at start-up (its own pool
+ * holds the rest of the device, so a cudaMalloc fails or takes memory the
+ * budget does not have), and latency-bound loops that cannot take the latency
+ * of cudaMalloc/cudaFree or the device-wide synchronisation cudaFree implies.
+ * This call allocates no device memory; the model must already exist.
+ *
+ * Runs the vote pass of ppf_model_lookup for one scene whose points and
+ * normals (n_scene x 3 float32 each) are device memory, with the model's
+ * d_dist as ppf_registration uses, and writes vote cells (code = s_r<<32 |
+ * m_r<<6 | alpha, as ppf_model_all_votes) and their counts to the caller's
+ * device arrays codes / counts (capacity entries each), in no particular
+ * order.  vote_floor >= 0: every cell whose count exceeds vote_floor (0 gives
+ * the nonzero cells ppf_model_all_votes returns).  vote_floor < 0: the
+ * lookup's candidates, every cell whose count exceeds the model's
+ * vote_count_threshold x the running maximum when its work item finished, a
+ * superset of the cells the lookup keeps (count >= threshold x *max_count),
+ * whose size varies from call to call.  *n_out: cells written;
+ * *max_count (may be NULL): the largest count.
+ *
+ * Scratch: counters, the work items that did not fit and the scene packed to
+ * float4 live in one static device array of 3 MiB + 256 B in the library,
+ * which every GPU that loads the library holds until the process exits.
+ * Limits: n_scene <= 65536 points and ceil(n_scene / ref_point_df) x model
+ * chunks <= 262144 work items (a model of n points has ceil(n / 1659) chunks
+ * on a B200); larger inputs return PPF_ERR_INVALID_ARGUMENT before any GPU
+ * work.  The call zeroes the scratch's 256-byte counter header on the
+ * context's stream before its kernels; nothing the caller passes needs to
+ * start at zero.  Output too small: PPF_ERR_OUT_OF_MEMORY, *n_out = the cells
+ * this call needed (the cells of the work items that fit were written).
+ *
+ * The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  All calls on one device share the array:
+ * calls that overlap in time (other threads, contexts or streams on the same
+ * device) race on it, so the caller serialises them.  Returns after the
+ * context's stream has finished the pass. */
+ppf_status ppf_model_vote_cells_noalloc(ppf_model_t m, const float* scene_xyz,
+                                        const float* scene_nxyz, uint64_t n_scene,
+                                        uint32_t ref_point_df, float vote_floor, uint64_t* codes,
+                                        uint32_t* counts, uint64_t capacity, uint64_t* n_out,
+                                        uint32_t* max_count);
+
 #ifdef __cplusplus
 }
 #endif

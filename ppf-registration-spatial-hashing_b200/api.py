@@ -253,6 +253,44 @@ class Model:
                                      counts.ctypes.data_as(_capi._u32p), n.value, C.byref(n)))
         return codes, counts
 
+    def vote_cells_noalloc(self, scene_xyz, scene_nxyz, ref_point_df: int, vote_floor: float,
+                           codes_out, counts_out):
+        """Allocation-free vote pass (ppf_model_vote_cells_noalloc; no reference counterpart).
+
+        For callers that may not allocate device memory while they run.  All
+        four arrays are the caller's CUDA tensors and are passed by pointer
+        with no copy or conversion: scene_xyz / scene_nxyz contiguous (n, 3)
+        float32, codes_out int64 / uint64 and counts_out int32 / uint32 of equal
+        length.  Writes the vote cells to the front of the outputs in no
+        particular order and returns (n_cells, max_count).  An output that is
+        too small raises PPFError (PPF_ERR_OUT_OF_MEMORY) whose ``needed``
+        attribute is the number of cells the call needed.  Calls on one device
+        share the library's static scratch array and must not overlap.
+        """
+        for name, t, dt in (("scene_xyz", scene_xyz, ("torch.float32",)),
+                            ("scene_nxyz", scene_nxyz, ("torch.float32",)),
+                            ("codes_out", codes_out, ("torch.int64", "torch.uint64")),
+                            ("counts_out", counts_out, ("torch.int32", "torch.uint32"))):
+            if not (hasattr(t, "is_cuda") and t.is_cuda and t.is_contiguous() and repr(t.dtype) in dt):
+                raise ValueError(f"{name}: expected a contiguous CUDA tensor of {' or '.join(dt)}")
+        if scene_xyz.shape != scene_nxyz.shape or scene_xyz.dim() != 2 or scene_xyz.shape[1] != 3:
+            raise ValueError("scene_xyz / scene_nxyz: expected two (n, 3) tensors")
+        if codes_out.numel() != counts_out.numel():
+            raise ValueError("codes_out and counts_out must have the same length")
+        n = C.c_uint64()
+        mx = C.c_uint32()
+        status = _lib().ppf_model_vote_cells_noalloc(
+            self.handle, C.c_void_p(scene_xyz.data_ptr()), C.c_void_p(scene_nxyz.data_ptr()),
+            int(scene_xyz.shape[0]), int(ref_point_df), float(vote_floor),
+            C.c_void_p(codes_out.data_ptr()), C.c_void_p(counts_out.data_ptr()),
+            int(codes_out.numel()), C.byref(n), C.byref(mx))
+        if status != _capi.PPF_OK:
+            msg = _lib().ppf_last_error()
+            err = PPFError(status, msg.decode() if msg else "")
+            err.needed = int(n.value)
+            raise err
+        return int(n.value), int(mx.value)
+
     def pair_vote_counts(self, scene: Scene) -> np.ndarray:
         out = np.zeros(scene.n * scene.n, np.uint64)
         _check(_lib().ppf_model_pair_vote_counts(self.handle, scene.handle, C.c_void_p(out.ctypes.data)))

@@ -459,6 +459,21 @@ ppf_status ppf_model_all_votes(ppf_model_t m, ppf_scene_t s, uint64_t* codes, ui
   });
 }
 
+ppf_status ppf_model_vote_cells_noalloc(ppf_model_t m, const float* scene_xyz,
+                                        const float* scene_nxyz, uint64_t n_scene,
+                                        uint32_t ref_point_df, float vote_floor, uint64_t* codes,
+                                        uint32_t* counts, uint64_t capacity, uint64_t* n_out,
+                                        uint32_t* max_count) {
+  return guarded([&]() {
+    PPF_REQUIRE(m && n_out, PPF_ERR_INVALID_ARGUMENT, "null model or count");
+    Context& c = *m->m.ctx;
+    PPF_CUDA(cudaSetDevice(c.device));
+    vote_cells_noalloc(c, m->m, scene_xyz, scene_nxyz, n_scene, ref_point_df, vote_floor, codes,
+                       counts, capacity, n_out, max_count);
+    return PPF_OK;
+  });
+}
+
 ppf_status ppf_model_pair_vote_counts(ppf_model_t m, ppf_scene_t s, uint64_t* counts) {
   return guarded([&]() {
     PPF_REQUIRE(m && s && counts, PPF_ERR_INVALID_ARGUMENT, "null model, scene or counts");

@@ -133,6 +133,12 @@ struct VoteResult {
 // ctx.cand_codes / ctx.cand_counts.
 VoteResult run_votes(Context& ctx, const Model& m, const SceneData& s, bool emit_all, float floor);
 void pair_vote_counts(Context& ctx, const Model& m, const SceneData& s, uint64_t* out_dev);
+// The vote pass with no device allocation: scene and outputs are the
+// caller's device arrays, everything else lives in a static device array of
+// vote.cu (ppf_model_vote_cells_noalloc).
+void vote_cells_noalloc(Context& ctx, const Model& m, const float* xyz, const float* nxyz,
+                        uint64_t n, uint32_t ref_df, float vote_floor, uint64_t* codes,
+                        uint32_t* counts, uint64_t capacity, uint64_t* n_out, uint32_t* max_out);
 
 // ---- poses and clustering (pose.cu)
 // Filters the candidates to the kept votes and orders them (count desc,

@@ -16,6 +16,8 @@
 // maximum: a superset of the cells the final threshold (threshold x global
 // maximum) keeps.
 #include <cstring>
+#include <mutex>
+#include <string>
 
 #include "engine.h"
 #include "ppf_math.cuh"
@@ -604,6 +606,151 @@ void pair_vote_counts(Context& ctx, const Model& m, const SceneData& s, uint64_t
   pair_vote_counts_kernel<<<grid, 256, 0, ctx.stream>>>(a, reinterpret_cast<unsigned long long*>(out_dev));
   PPF_CUDA(cudaGetLastError());
   ctx.launches++;
+}
+
+// ---- allocation-free vote pass (ppf_model_vote_cells_noalloc)
+//
+// The same vote kernel as run_votes, for callers that must not allocate
+// device memory while they run: a serving process whose device-memory budget
+// was reserved at start-up (its own pool holds the rest of the device, so a
+// further cudaMalloc fails or takes memory the budget does not have) and
+// latency-bound loops that cannot take cudaMalloc/cudaFree latency or the
+// device-wide synchronisation that cudaFree implies.  Everything the pass
+// needs besides the caller's inputs and outputs lives in one static device
+// array of this file, which every GPU that loads the library holds until the
+// process exits:
+//   [0, 256)        counters (the run_votes layout), the flags word at byte
+//                   64 and the bad-index record at byte 96
+//   items           the work items that did not fit the caller's output
+//   points, normals the scene packed to float4
+constexpr uint32_t kNoAllocMaxScenePoints = 65536;
+constexpr uint32_t kNoAllocMaxItems = 262144;  // scene reference points x model chunks
+constexpr size_t kNoAllocHeader = 256;
+constexpr size_t kNoAllocItemsOff = kNoAllocHeader;
+constexpr size_t kNoAllocPtsOff = kNoAllocItemsOff + (size_t)kNoAllocMaxItems * 4;
+constexpr size_t kNoAllocNrmOff = kNoAllocPtsOff + (size_t)kNoAllocMaxScenePoints * 16;
+constexpr size_t kNoAllocBytes = kNoAllocNrmOff + (size_t)kNoAllocMaxScenePoints * 16;  // 3 MiB + 256 B
+static_assert(kNoAllocPtsOff % 256 == 0 && kNoAllocNrmOff % 256 == 0, "scratch sections stay aligned");
+
+static __device__ __align__(256) unsigned char g_vote_scratch[kNoAllocBytes];
+
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_vote_scratch_mutex;
+unsigned char* g_vote_scratch_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of g_vote_scratch on `device`, which must be current.  The
+// first call per device looks it up; later calls reuse it.
+unsigned char* vote_scratch(int device) {
+  PPF_REQUIRE(device >= 0 && device < kNoAllocMaxDevices, PPF_ERR_INVALID_ARGUMENT,
+              "device index beyond the allocation-free path's table of 64 devices");
+  std::lock_guard<std::mutex> lock(g_vote_scratch_mutex);
+  if (!g_vote_scratch_ptr[device]) {
+    void* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_vote_scratch);
+    if (e != cudaSuccess || !ptr)
+      throw Error(PPF_ERR_CUDA, std::string("cudaGetSymbolAddress(vote scratch): ") + cudaGetErrorString(e));
+    g_vote_scratch_ptr[device] = static_cast<unsigned char*>(ptr);
+  }
+  return g_vote_scratch_ptr[device];
+}
+
+__global__ void pack_scene_kernel(const float* __restrict__ xyz, const float* __restrict__ nxyz,
+                                  uint32_t n, float4* __restrict__ pts, float4* __restrict__ nrm) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    pts[i] = make_float4(xyz[3 * (size_t)i], xyz[3 * (size_t)i + 1], xyz[3 * (size_t)i + 2], 0.f);
+    nrm[i] = make_float4(nxyz[3 * (size_t)i], nxyz[3 * (size_t)i + 1], nxyz[3 * (size_t)i + 2], 0.f);
+  }
+}
+
+}  // namespace
+
+void vote_cells_noalloc(Context& ctx, const Model& m, const float* xyz, const float* nxyz,
+                        uint64_t n, uint32_t ref_df, float vote_floor, uint64_t* codes,
+                        uint32_t* counts, uint64_t capacity, uint64_t* n_out, uint32_t* max_out) {
+  *n_out = 0;
+  if (max_out) *max_out = 0;
+  PPF_REQUIRE(n <= kNoAllocMaxScenePoints, PPF_ERR_INVALID_ARGUMENT,
+              "scene of " + std::to_string(n) + " points exceeds the allocation-free limit of " +
+                  std::to_string(kNoAllocMaxScenePoints));
+  if (n < 2) return;
+  PPF_REQUIRE(xyz && nxyz && is_device_pointer(xyz) && is_device_pointer(nxyz),
+              PPF_ERR_INVALID_ARGUMENT, "scene points and normals must be device memory");
+  PPF_REQUIRE(capacity == 0 || (codes && counts && is_device_pointer(codes) && is_device_pointer(counts)),
+              PPF_ERR_INVALID_ARGUMENT, "vote cell outputs must be device memory");
+  PPF_REQUIRE(capacity <= 0xffffffffull, PPF_ERR_INVALID_ARGUMENT, "capacity beyond 2^32 - 1 cells");
+  ref_df = ref_df ? ref_df : 1;
+  const uint64_t n_ref = (n + ref_df - 1) / ref_df;
+  const uint64_t n_items = n_ref * m.t.n_chunks;
+  PPF_REQUIRE(n_items <= kNoAllocMaxItems, PPF_ERR_INVALID_ARGUMENT,
+              std::to_string(n_ref) + " scene reference points x " + std::to_string(m.t.n_chunks) +
+                  " model chunks exceed the allocation-free limit of " + std::to_string(kNoAllocMaxItems) +
+                  " work items");
+  const size_t smem = kVoteQueueBytes + vote_acc_words(m.t.chunk) * 4;
+  PPF_REQUIRE((int)smem <= ctx.vote_smem_limit, PPF_ERR_INTERNAL, "vote accumulator too large");
+
+  unsigned char* scratch = vote_scratch(ctx.device);
+  cudaStream_t stream = ctx.stream;
+  float4* pts = reinterpret_cast<float4*>(scratch + kNoAllocPtsOff);
+  float4* nrm = reinterpret_cast<float4*>(scratch + kNoAllocNrmOff);
+  // the counter header is the only part of the scratch that must start at zero
+  PPF_CUDA(cudaMemsetAsync(scratch, 0, kNoAllocHeader, stream));
+  pack_scene_kernel<<<grid_for(n, 256), 256, 0, stream>>>(xyz, nxyz, (uint32_t)n, pts, nrm);
+  PPF_CUDA(cudaGetLastError());
+  ctx.launches++;
+
+  // scene with no storage of its own: make_args takes n, d_dist and ref_df from it
+  SceneData s;
+  s.n = (uint32_t)n;
+  s.d_dist = m.t.d_dist;  // ppf_registration builds each scene with its model's d_dist
+  s.ref_df = ref_df;
+  VoteArgs a = make_args(m, s);
+  a.s_pts = pts;
+  a.s_nrm = nrm;
+  a.emit_all = 0;
+  a.floor = vote_floor;
+  uint32_t* cnt = reinterpret_cast<uint32_t*>(scratch);
+  a.work_counter = cnt + 0;
+  a.global_max = cnt + 1;
+  a.n_cand = cnt + 2;
+  a.n_redo = cnt + 3;
+  a.stats = reinterpret_cast<unsigned long long*>(cnt + 4);
+  a.n_needed = reinterpret_cast<unsigned long long*>(cnt + 10);
+  a.flags = cnt + 16;
+  a.bad = reinterpret_cast<unsigned long long*>(cnt + 24);
+  a.cand_code = reinterpret_cast<unsigned long long*>(codes);
+  a.cand_count = counts;
+  a.cand_cap = (uint32_t)capacity;
+  a.redo_items = reinterpret_cast<uint32_t*>(scratch + kNoAllocItemsOff);
+  a.n_items_total = kNoAllocMaxItems;
+  a.item_list = nullptr;
+  a.n_items = (uint32_t)n_items;
+  auto kernel = ctx.checks ? vote_kernel<true> : vote_kernel<false>;
+  PPF_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kernel<<<(unsigned)std::min<uint64_t>(n_items, (uint64_t)sm_count()), kVoteThreads, smem, stream>>>(a);
+  PPF_CUDA(cudaGetLastError());
+  ctx.launches++;
+
+  unsigned long long h[22];  // bytes [0, 176): counters, flags, bad-index record
+  PPF_CUDA(cudaMemcpyAsync(h, scratch, sizeof(h), cudaMemcpyDeviceToHost, stream));
+  PPF_CUDA(cudaStreamSynchronize(stream));
+  const uint32_t* h32 = reinterpret_cast<const uint32_t*>(h);
+  if (h32[16] & kFlagBadIndex) {
+    const unsigned long long* bad = h + 12;
+    throw Error(PPF_ERR_INTERNAL, "vote kernel index out of range: site " + std::to_string(bad[0]) +
+                                      " value " + std::to_string(bad[1]) + " bound " +
+                                      std::to_string(bad[2]));
+  }
+  if (max_out) *max_out = h32[1];
+  if (h32[3]) {
+    const unsigned long long needed = h[5];
+    *n_out = needed;
+    throw Error(PPF_ERR_OUT_OF_MEMORY,
+                "vote cell output of " + std::to_string(capacity) + " entries is too small: this call needed " +
+                    std::to_string(needed) + " (the cells of the items that fit were written)");
+  }
+  *n_out = h32[2];
 }
 
 }  // namespace ppf
