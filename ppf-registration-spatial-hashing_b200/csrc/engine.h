@@ -98,6 +98,7 @@ struct LookupState {
   DevBuf cells3;      // int4 U: integer cell of each pose
   DevBuf qs, tws, adjrun, item_off;  // cell-major clustering tables
   DevBuf tmp64, tmp32a, tmp32b, perm;
+  DevBuf tperm;       // clustering target order (cell, rotation bucket)
   DevBuf best;        // float[16] pose + int idx
   std::vector<float> cpu_poses;
 };

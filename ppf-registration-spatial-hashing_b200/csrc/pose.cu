@@ -208,25 +208,44 @@ __global__ void gather_sorted_kernel(const uint32_t* __restrict__ map, size_t U,
   }
 }
 
-// Per cell run: its 27 neighbour runs (-1: none / the centre), the number of
-// target tiles, and whether all its poses share one int3 cell (two cells with
-// one hash would need per-pose neighbour lists).
+// Whether two different int3 cells share one cell key (then the per-pose
+// neighbour lists of cluster_kernel are needed): a sorted position whose key
+// equals its predecessor's but whose cell differs.
+__global__ void mixed_cells_kernel(const uint32_t* __restrict__ sorted_keys, const uint32_t* __restrict__ map,
+                                   const int4* __restrict__ cells3, size_t U, uint32_t* __restrict__ mixed) {
+  for (size_t p = 1 + blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < U;
+       p += (size_t)gridDim.x * blockDim.x) {
+    if (sorted_keys[p] != sorted_keys[p - 1]) continue;
+    const int4 c = cells3[map[p]], c0 = cells3[map[p - 1]];
+    if (c.x != c0.x || c.y != c0.y || c.z != c0.z) atomicOr(mixed, 1u);
+  }
+}
+
+// 4-D grid bucket of a unit quaternion, 16 cells of 0.125 per component.
+__device__ __forceinline__ uint32_t quat_bucket(float4 q) {
+  auto b = [](float x) { return (uint32_t)min(max(__float2int_rd((x + 1.f) * 8.f), 0), 15); };
+  return (b(q.w) << 12) | (b(q.z) << 8) | (b(q.y) << 4) | b(q.x);
+}
+
+// Sort key of each pose as a clustering target: its cell key, then its
+// rotation bucket, so the 32 targets of a warp hold similar rotations.
+__global__ void target_keys_kernel(const uint32_t* __restrict__ sorted_keys, const float4* __restrict__ qs,
+                                   size_t U, unsigned long long* __restrict__ keys) {
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < U;
+       p += (size_t)gridDim.x * blockDim.x)
+    keys[p] = ((unsigned long long)sorted_keys[p] << 16) | quat_bucket(qs[p]);
+}
+
+// Per cell run: its 27 neighbour runs (-1: none / the centre) and the number
+// of target tiles.
 __global__ void run_adjacency_kernel(const uint32_t* __restrict__ first, const uint32_t* __restrict__ count,
                                      size_t Kc, const uint32_t* __restrict__ map,
                                      const int4* __restrict__ cells3, const uint32_t* __restrict__ uniq,
-                                     int* __restrict__ adjrun, uint32_t* __restrict__ tiles,
-                                     uint32_t* __restrict__ mixed) {
+                                     int* __restrict__ adjrun, uint32_t* __restrict__ tiles) {
   for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < Kc;
        r += (size_t)gridDim.x * blockDim.x) {
     const uint32_t f = first[r], n = count[r];
     const int4 c0 = cells3[map[f]];
-    for (uint32_t e = 1; e < n; ++e) {
-      int4 c = cells3[map[f + e]];
-      if (c.x != c0.x || c.y != c0.y || c.z != c0.z) {
-        atomicOr(mixed, 1u);
-        break;
-      }
-    }
     int b = 0;
     for (int di = -1; di < 2; ++di)
       for (int dj = -1; dj < 2; ++dj)
@@ -252,6 +271,7 @@ struct TiledArgs {
   const uint32_t* first;
   const uint32_t* count;
   const uint32_t* map;
+  const uint32_t* tperm;  // target order: positions sorted by (cell, rotation bucket)
   const int* adjrun;
   const uint32_t* item_off;  // exclusive scan of tiles per run
   size_t Kc;
@@ -264,9 +284,33 @@ struct TiledArgs {
   float* trans;
 };
 
+__device__ __forceinline__ float warp_min(float v) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Scores of rot_clustering_kernel (src/cuda/kernel.cu:702-763), cell-major.
+// A block takes a tile of up to 256 targets of one cell, ordered by rotation
+// bucket, and streams the poses of the cell's neighbour cells through shared
+// memory in the reference's order (neighbour b = 0..26, then position).  Each
+// warp first marks, with one ballot per 32 sources, the sources inside a box
+// around its targets: quaternion components within 0.25 of some target's
+// (the rotation test implies a quaternion distance below 2*pi/30 < 0.21) and,
+// in L2 mode, translation components within 1.0001 d_dist.  It then runs the
+// reference's tests on the marked sources only, in ascending order, so every
+// target adds the same weights in the same order as the reference.
 __global__ void __launch_bounds__(kClusterTile) cluster_tiled_kernel(TiledArgs a) {
   __shared__ float4 sq[kClusterTile], stw[kClusterTile];
   const float rot_sq = PPF_ROT_THRESH * PPF_ROT_THRESH;
+  const int lane = threadIdx.x & 31;
+  constexpr float kQuatMargin = 0.25f;
+  const float t_margin = a.use_l1 ? INFINITY : a.d_dist * 1.0001f + 1e-6f;
   for (uint32_t item = blockIdx.x; item < a.n_items; item += gridDim.x) {
     size_t lo = 0, hi = a.Kc;  // run r with item_off[r] <= item < item_off[r + 1]
     while (hi - lo > 1) {
@@ -275,14 +319,30 @@ __global__ void __launch_bounds__(kClusterTile) cluster_tiled_kernel(TiledArgs a
       else hi = mid;
     }
     const size_t r = lo;
-    const uint32_t p = a.first[r] + (item - a.item_off[r]) * kClusterTile + threadIdx.x;
-    const bool valid = p < a.first[r] + a.count[r];
+    const uint32_t slot = a.first[r] + (item - a.item_off[r]) * kClusterTile + threadIdx.x;
+    const bool valid = slot < a.first[r] + a.count[r];
+    const uint32_t p = valid ? a.tperm[slot] : 0u;
     float4 q = make_float4(0, 0, 0, 0), tw = make_float4(0, 0, 0, 0);
     if (valid) {
       q = a.qs[p];
       tw = a.tws[p];
     }
     const float3 t = make_float3(tw.x, tw.y, tw.z);
+    // the warp's box (empty for a warp without targets)
+    const float4 qlo = make_float4(warp_min(valid ? q.x : INFINITY) - kQuatMargin,
+                                   warp_min(valid ? q.y : INFINITY) - kQuatMargin,
+                                   warp_min(valid ? q.z : INFINITY) - kQuatMargin,
+                                   warp_min(valid ? q.w : INFINITY) - kQuatMargin);
+    const float4 qhi = make_float4(warp_max(valid ? q.x : -INFINITY) + kQuatMargin,
+                                   warp_max(valid ? q.y : -INFINITY) + kQuatMargin,
+                                   warp_max(valid ? q.z : -INFINITY) + kQuatMargin,
+                                   warp_max(valid ? q.w : -INFINITY) + kQuatMargin);
+    const float3 tlo = make_float3(warp_min(valid ? t.x : INFINITY) - t_margin,
+                                   warp_min(valid ? t.y : INFINITY) - t_margin,
+                                   warp_min(valid ? t.z : INFINITY) - t_margin);
+    const float3 thi = make_float3(warp_max(valid ? t.x : -INFINITY) + t_margin,
+                                   warp_max(valid ? t.y : -INFINITY) + t_margin,
+                                   warp_max(valid ? t.z : -INFINITY) + t_margin);
     float c = 1;
     float3 to = t;
     for (int b = 0; b < 27; ++b) {
@@ -296,23 +356,36 @@ __global__ void __launch_bounds__(kClusterTile) cluster_tiled_kernel(TiledArgs a
           stw[threadIdx.x] = a.tws[f + s0 + threadIdx.x];
         }
         __syncthreads();
-        if (!valid) continue;
         const uint32_t m = min((uint32_t)kClusterTile, n - s0);
-        for (uint32_t jj = 0; jj < m; ++jj) {
-          const float qd = fabsf(8 * (1 - dot4(q, sq[jj])));
-          if (qd < rot_sq) {
-            const float4 sj = stw[jj];
-            const float3 tj = make_float3(sj.x, sj.y, sj.z);
-            if (!a.use_l1) {
-              float nd = norm3(v3_sub(t, tj));
-              if (!(nd < a.d_dist)) continue;
+        for (uint32_t j0 = 0; j0 < m; j0 += 32) {
+          const uint32_t jl = j0 + lane;
+          bool in = false;
+          if (jl < m) {
+            const float4 sj = sq[jl], wj = stw[jl];
+            in = sj.x >= qlo.x && sj.x <= qhi.x && sj.y >= qlo.y && sj.y <= qhi.y && sj.z >= qlo.z &&
+                 sj.z <= qhi.z && sj.w >= qlo.w && sj.w <= qhi.w && wj.x >= tlo.x && wj.x <= thi.x &&
+                 wj.y >= tlo.y && wj.y <= thi.y && wj.z >= tlo.z && wj.z <= thi.z;
+          }
+          uint32_t mask = __ballot_sync(0xffffffffu, in);
+          while (mask) {
+            const uint32_t jj = j0 + (uint32_t)(__ffs(mask) - 1);
+            mask &= mask - 1;
+            if (!valid) continue;
+            const float qd = fabsf(8 * (1 - dot4(q, sq[jj])));
+            if (qd < rot_sq) {
+              const float4 sj = stw[jj];
+              const float3 tj = make_float3(sj.x, sj.y, sj.z);
+              if (!a.use_l1) {
+                float nd = norm3(v3_sub(t, tj));
+                if (!(nd < a.d_dist)) continue;
+              }
+              if (a.use_avg) {
+                to = v3_scale(c, to);
+                to = v3_add(to, v3_scale(sj.w, tj));
+                to = v3_scale(1 / (c + sj.w), to);
+              }
+              c += sj.w;
             }
-            if (a.use_avg) {
-              to = v3_scale(c, to);
-              to = v3_add(to, v3_scale(sj.w, tj));
-              to = v3_scale(1 / (c + sj.w), to);
-            }
-            c += sj.w;
           }
         }
       }
@@ -517,17 +590,27 @@ size_t cluster_poses_gpu(Context& ctx, const Model& m, LookupState& st, float* b
   PPF_CUDA(cudaMemsetAsync(ctx.counters.ptr, 0, 8, stream));
   uint32_t* mixed = ctx.counters.as<uint32_t>();
   gather_sorted_kernel<<<grid_for(U, 256), 256, 0, stream>>>(map, U, a.quats, a.trans0, a.weighted, qs, tws);
+  mixed_cells_kernel<<<grid_for(U, 256), 256, 0, stream>>>(ck, map, st.cells3.as<int4>(), U, mixed);
   run_adjacency_kernel<<<grid_for(Kc, 128), 128, 0, stream>>>(fi, ct, Kc, map, st.cells3.as<int4>(), uq,
-                                                              adjrun, item_off, mixed);
+                                                              adjrun, item_off);
   exclusive_scan_small(item_off, Kc, mixed + 1, stream);
   uint32_t hc[2];
   PPF_CUDA(cudaMemcpyAsync(hc, mixed, 8, cudaMemcpyDeviceToHost, stream));
   PPF_CUDA(cudaStreamSynchronize(stream));
-  ctx.launches += 3;
+  ctx.launches += 4;
   if (hc[0]) {
     cluster_kernel<<<grid_for(U, 128), 128, 0, stream>>>(a);
   } else {
+    // targets of each cell ordered by rotation bucket
+    unsigned long long* tkeys = grow<unsigned long long>(st.tmp64, U);
+    uint32_t* tperm = grow<uint32_t>(st.tperm, U);
+    target_keys_kernel<<<grid_for(U, 256), 256, 0, stream>>>(ck, qs, U, tkeys);
+    ctx.launches++;
+    const size_t l1 = ctx.sort64.launches();
+    ctx.sort64.sort(tkeys, tperm, true, U, 0, 48, stream, ctx.flags.as<uint32_t>());
+    ctx.launches += ctx.sort64.launches() - l1;
     TiledArgs ta;
+    ta.tperm = tperm;
     ta.first = fi;
     ta.count = ct;
     ta.map = map;
