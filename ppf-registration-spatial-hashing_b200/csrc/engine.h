@@ -59,7 +59,7 @@ struct ModelTables {
   size_t P = 0;
   DevBuf keys;           // uint32 sorted keys
   DevBuf pairs;          // uint32 pair index r*n + i (the hash array's data map)
-  DevBuf entries;        // uint32 ((m_r mod chunk) * 31) << 16 | 16-bit angle of u,
+  DevBuf entries;        // uint32 (m_r mod chunk) << 21 | 21-bit angle of u,
                          // vote order: by key, then m_r, then a hash of the pair
   DevBuf epairs;         // uint32 pair index of each entry (vote order)
   // runs

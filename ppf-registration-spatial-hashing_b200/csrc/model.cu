@@ -70,10 +70,10 @@ __global__ void order_words_kernel(const uint32_t* __restrict__ keys, const uint
   }
 }
 
-// Vote entry of each pair in vote order: ((m_r mod chunk) * 31) << 16 |
-// angle16(u), u = the pair's second point in the frame of the first: the high
-// half is the pair's accumulator row inside its m_r chunk, so the vote kernel
-// forms a cell index with one add.  A pair whose u is
+// Vote entry of each pair in vote order: (m_r mod chunk) << 21 | angle21(u),
+// u = the pair's second point in the frame of the first: the top 11 bits are
+// the pair's m_r inside its chunk, so the vote kernel forms the cell index
+// row * 31 + bin with one multiply-add.  A pair whose u is
 // (numerically) zero cannot be binned from angles; its run is flagged for
 // exact binning.
 __global__ void entries_kernel(const uint32_t* __restrict__ epairs, size_t P, uint32_t n,
@@ -90,7 +90,7 @@ __global__ void entries_kernel(const uint32_t* __restrict__ epairs, size_t P, ui
     f.r2 = r2[mr];
     float4 q4 = pts[mi];
     float2 u = frame_point_yz(f, make_float3(q4.x, q4.y, q4.z));
-    entries[j] = (((mr % chunk) * (uint32_t)PPF_N_ANGLE_CELLS) << 16) | angle16(u);
+    entries[j] = ((mr % chunk) << PPF_ANGLE_BITS) | angle21(u);
     if (fabsf(u.x) + fabsf(u.y) < 1e-12f || !isfinite(u.x) || !isfinite(u.y)) {
       // run of position j: last run start <= j
       size_t lo = 0, hi = K;
@@ -170,7 +170,7 @@ __global__ void validate_tables_kernel(const uint32_t* __restrict__ keys, size_t
     const uint32_t pr = epairs[j];
     if (pr >= (uint32_t)(n * n)) report(102, j);
     const uint32_t mr = pr / n;
-    if ((entries[j] >> 16) != (mr % chunk) * (uint32_t)kBins) report(103, j);
+    if ((entries[j] >> PPF_ANGLE_BITS) != mr % chunk) report(103, j);
   }
   for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < K;
        r += (size_t)gridDim.x * blockDim.x) {
@@ -291,9 +291,9 @@ void build_model(Context& ctx, ModelTables& t, const float* xyz, const float* nx
 
   // m_r chunks sized to the vote kernel's shared-memory accumulator
   uint32_t max_chunk = 64;
-  // (a chunk's accumulator row offsets, (m_r mod chunk) * 31, fit 16 bits)
+  // (m_r mod chunk fits the 11 bits above an entry's 21-bit angle)
   while (vote_acc_words(max_chunk + 1) * 4 + kVoteQueueBytes <= (size_t)ctx.vote_smem_limit &&
-         max_chunk * (uint32_t)kBins < 65536u - kBins)
+         max_chunk < (1u << (32 - PPF_ANGLE_BITS)))
     ++max_chunk;
   t.n_chunks = (t.n + max_chunk - 1) / max_chunk;
   t.chunk = (t.n + t.n_chunks - 1) / t.n_chunks;

@@ -305,33 +305,26 @@ __device__ __forceinline__ unsigned alpha_bin_exact(float2 u, float2 v) {
   return alpha_bin_of(alpha_angle(u, v));
 }
 
-// 16-bit fixed-point direction angle of (y, z): round(atan2(z, y) * 2^16 / 2pi).
-// Used by the fast bin path; the error is at most 0.51 units of 2pi/2^16.
-__device__ __forceinline__ uint32_t angle16(float2 yz) {
+// 21-bit fixed-point direction angle of (y, z): round(atan2(z, y) * 2^21 / 2pi)
+// mod 2^21, in units of 2pi / 2^21 (3.0e-6 rad).  Error against the exact
+// angle of the float vector: 0.5 units of rounding, atan2f's few ulp of pi
+// (0.23 units) and the scaling multiply (0.12 units): under 0.9 units.
+__device__ __forceinline__ uint32_t angle21(float2 yz) {
   float a = atan2f(yz.y, yz.x);  // [-pi, pi]
-  float s = a * (65536.0f / (2.0f * CUDART_PI_F));
+  float s = a * (2097152.0f / (2.0f * CUDART_PI_F));
   int q = __float2int_rn(s);
-  return (uint32_t)q & 0xffffu;
+  return (uint32_t)q & 0x1fffffu;
 }
 
-// Fast alpha bin from the 16-bit angles of u (model) and v (scene).
-//   alpha = beta_v - beta_u, x = alpha + pi, bin = floor(x * 30 / 2pi).
-// The reference's x differs from the exact angle difference of the float
-// vectors by at most ~1.5e-6 rad (rounding of cross/dot, atan2f's 3-ulp
-// bound, the add of pi); the 16-bit angles add at most 2 x 0.51 units.
-// Positions closer than kMarginUnits units to a bin edge (including the
-// wrap at x = 0 / 2pi) are reported as ambiguous and must take the exact
-// path.  Returns the bin, or -1 when ambiguous.
-#define PPF_BIN_MARGIN_UNITS 2
-__device__ __forceinline__ int alpha_bin_fast(uint32_t beta_u, uint32_t beta_v) {
-  uint32_t x = (beta_v - beta_u + 32768u) & 0xffffu;
-  uint32_t t = x * (uint32_t)PPF_N_ANGLE;  // bin * 65536 + residue
-  uint32_t r = t & 0xffffu;
-  // residue within margin*30 of a boundary -> ambiguous
-  const uint32_t m = PPF_BIN_MARGIN_UNITS * PPF_N_ANGLE;
-  if (r < m || r > 65536u - m) return -1;
-  return (int)(t >> 16);
-}
+// Fast alpha bin from the 21-bit angles beta_m of u (model) and beta_s of v
+// (scene): alpha + pi = beta_s - beta_m + 2^20 units, bin = floor(30 x /
+// 2^21).  The reference's alpha + pi differs from the exact angle difference
+// of the float vectors by at most ~1.5e-6 rad (0.5 units: rounding of the
+// cross and dot products, atan2f's bound, the add of pi), and the two 21-bit
+// angles add under 1.8 units, so a vote within PPF_BIN_MARGIN_UNITS of a bin
+// edge (including the wrap at 0 / 2pi) is ambiguous and takes the exact path.
+#define PPF_BIN_MARGIN_UNITS 6
+#define PPF_ANGLE_BITS 21
 
 // --------------------------------------------------------------- poses --
 

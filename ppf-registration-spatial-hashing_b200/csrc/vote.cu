@@ -28,6 +28,7 @@ namespace {
 constexpr uint32_t kSeg = 1024;   // entries per segment
 constexpr int kUnroll = 8;        // independent entry loads per lane
 constexpr uint32_t kNoRun = 0xffffffffu;
+constexpr uint32_t kExactOnly = 1u << 31;  // scene angle flag: every vote of the pair takes the exact path
 
 struct VoteArgs {
   // model
@@ -224,7 +225,7 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
             if (len) {
               v = frame_point_yz(fs, pi);
               bool degenerate = fabsf(v.x) + fabsf(v.y) < 1e-12f || !isfinite(v.x) || !isfinite(v.y);
-              beta = angle16(v) | ((degenerate || __ldg(a.run_flags + run)) ? 0x10000u : 0u);
+              beta = angle21(v) | ((degenerate || __ldg(a.run_flags + run)) ? kExactOnly : 0u);
             }
           }
         }
@@ -278,21 +279,23 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
           end = start;
         }
         const uint32_t bw = q_beta[p];
-        const uint32_t bsp = bw + 32768u;  // bits above 16 shift out below
         const float2 vv = q_v[p];
-        // Each entry holds its accumulator row (m_r - mr_lo) * 31 in the high
-        // half and the model angle beta_m in the low half.  With y = (beta_s +
-        // 2^15 - beta_m) << 16, i.e. alpha + pi in 2^-32 turns, the bin is the
-        // high word of y * 30 and the low word is the position inside the bin.
-        const uint32_t bsh = bsp << 16;
-        constexpr uint32_t m_lo = (PPF_BIN_MARGIN_UNITS * PPF_N_ANGLE) << 16;
-        constexpr uint32_t m_span = (65536u - 2 * PPF_BIN_MARGIN_UNITS * PPF_N_ANGLE) << 16;
+        // Each entry holds the pair's m_r inside the chunk in its top 11 bits
+        // and the model angle beta_m in its low 21.  With y = (beta_s + 2^20 -
+        // beta_m) << 11, i.e. alpha + pi in 2^-32 turns (the row bits and the
+        // exact-only flag shift out), the bin is the high word of y * 30 and
+        // the low word is the position inside the bin.
+        constexpr int kShift = 32 - PPF_ANGLE_BITS;
+        const uint32_t bsh = (bw + (1u << (PPF_ANGLE_BITS - 1))) << kShift;
+        constexpr uint32_t m_lo = (PPF_BIN_MARGIN_UNITS * PPF_N_ANGLE) << kShift;
+        constexpr uint32_t m_span =
+            ((1u << PPF_ANGLE_BITS) - 2 * PPF_BIN_MARGIN_UNITS * PPF_N_ANGLE) << kShift;
         const uint32_t* ep = a.entries + start + lane;
         const uint32_t n_here = end - start;
-        if (bw & 0x10000u) {
+        if (bw & kExactOnly) {
           // degenerate frame vector or run: every vote takes the exact path
           for (uint32_t k = lane; k < n_here; k += 32) {
-            const uint32_t row = __ldg(a.entries + start + k) >> 16;
+            const uint32_t row = (__ldg(a.entries + start + k) >> PPF_ANGLE_BITS) * kBins;
             const uint32_t cell = row + exact_bin<kCheck>(a, start + k, vv);
             if (in_range<kCheck>(a, 6, cell, cells)) atomicAdd(&acc[cell], 1u);
             ++my_exact;
@@ -305,10 +308,11 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
             for (int u = 0; u < kUnroll; ++u) e[u] = __ldg(ep + 32 * u);
 #pragma unroll
             for (int u = 0; u < kUnroll; ++u) {
-              const uint32_t y = bsh - (e[u] << 16);
-              uint32_t cell = (e[u] >> 16) + __umulhi(y, (uint32_t)PPF_N_ANGLE);
+              const uint32_t y = bsh - (e[u] << kShift);
+              uint32_t cell = (e[u] >> PPF_ANGLE_BITS) * kBins + __umulhi(y, (uint32_t)PPF_N_ANGLE);
               if (y * (uint32_t)PPF_N_ANGLE - m_lo > m_span) {  // near a bin edge
-                cell = (e[u] >> 16) + exact_bin<kCheck>(a, (uint32_t)(ep + 32 * u - a.entries), vv);
+                cell = (e[u] >> PPF_ANGLE_BITS) * kBins +
+                       exact_bin<kCheck>(a, (uint32_t)(ep + 32 * u - a.entries), vv);
                 ++my_exact;
               }
               if (in_range<kCheck>(a, 7, cell, cells)) atomicAdd(&acc[cell], 1u);
@@ -316,10 +320,10 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
           }
           for (uint32_t k = nfull * 32 * kUnroll + lane; k < n_here; k += 32) {
             const uint32_t e = __ldg(a.entries + start + k);
-            const uint32_t y = bsh - (e << 16);
-            uint32_t cell = (e >> 16) + __umulhi(y, (uint32_t)PPF_N_ANGLE);
+            const uint32_t y = bsh - (e << kShift);
+            uint32_t cell = (e >> PPF_ANGLE_BITS) * kBins + __umulhi(y, (uint32_t)PPF_N_ANGLE);
             if (y * (uint32_t)PPF_N_ANGLE - m_lo > m_span) {
-              cell = (e >> 16) + exact_bin<kCheck>(a, start + k, vv);
+              cell = (e >> PPF_ANGLE_BITS) * kBins + exact_bin<kCheck>(a, start + k, vv);
               ++my_exact;
             }
             if (in_range<kCheck>(a, 8, cell, cells)) atomicAdd(&acc[cell], 1u);
