@@ -251,12 +251,11 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
       // ---- warps take segments; lanes stream consecutive entries
       uint32_t s = warp;
       while (s < n_seg_total) {
-        uint32_t plo = 0, phi = kVoteThreads;  // pair p with q_seg[p] <= s < q_seg[p+1]
-        while (phi - plo > 1) {
-          uint32_t mid = (plo + phi) >> 1;
-          if (q_seg[mid] <= s) plo = mid;
-          else phi = mid;
-        }
+        // pair p with q_seg[p] <= s < q_seg[p+1]: the last index whose segment
+        // offset is <= s (q_seg is nondecreasing and q_seg[0] = 0), found with
+        // two ballots: first over q_seg[32 l], then inside that block of 32
+        const uint32_t blk = 31u - __clz(__ballot_sync(0xffffffffu, q_seg[32 * lane] <= s));
+        const uint32_t plo = 32u * blk + 31u - __clz(__ballot_sync(0xffffffffu, q_seg[32 * blk + lane] <= s));
         const uint32_t p = plo;
         const uint32_t start = q_lo[p] + (s - q_seg[p]) * kSeg;
         uint32_t end = min(q_lo[p] + q_len[p], start + kSeg);
@@ -292,6 +291,23 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
             ((1u << PPF_ANGLE_BITS) - 2 * PPF_BIN_MARGIN_UNITS * PPF_N_ANGLE) << kShift;
         const uint32_t* ep = a.entries + start + lane;
         const uint32_t n_here = end - start;
+        // A vote near a bin edge was counted in its fast cell; move it to the
+        // cell of the reference's exact arithmetic (rare: ~1.7e-4 of votes).
+        auto fix_up = [&](uint32_t amb, const uint32_t* first_entry) {
+          for (int u = 0; amb; ++u, amb >>= 1) {
+            if (!(amb & 1u)) continue;
+            const uint32_t pos = (uint32_t)(first_entry + 32 * u - a.entries);
+            const uint32_t e = __ldg(a.entries + pos);
+            const uint32_t row = (e >> PPF_ANGLE_BITS) * kBins;
+            const uint32_t fast = row + __umulhi(bsh - (e << kShift), (uint32_t)PPF_N_ANGLE);
+            const uint32_t exact = row + exact_bin<kCheck>(a, pos, vv);
+            if (exact != fast && in_range<kCheck>(a, 7, exact, cells)) {
+              atomicAdd(&acc[fast], 0xffffffffu);
+              atomicAdd(&acc[exact], 1u);
+            }
+            ++my_exact;
+          }
+        };
         if (bw & kExactOnly) {
           // degenerate frame vector or run: every vote takes the exact path
           for (uint32_t k = lane; k < n_here; k += 32) {
@@ -301,22 +317,25 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
             ++my_exact;
           }
         } else {
+          // kUnroll entries per lane per pass, branch-free: the fast cell of
+          // every vote is counted, and the rare votes near a bin edge are
+          // moved afterwards.  The last pass is masked to the segment's end.
           const uint32_t nfull = n_here / (32 * kUnroll);
           for (uint32_t it = 0; it < nfull; ++it, ep += 32 * kUnroll) {
-            uint32_t e[kUnroll];
+            uint32_t c[kUnroll];
+            uint32_t amb = 0;
 #pragma unroll
-            for (int u = 0; u < kUnroll; ++u) e[u] = __ldg(ep + 32 * u);
+            for (int u = 0; u < kUnroll; ++u) c[u] = __ldg(ep + 32 * u);
 #pragma unroll
             for (int u = 0; u < kUnroll; ++u) {
-              const uint32_t y = bsh - (e[u] << kShift);
-              uint32_t cell = (e[u] >> PPF_ANGLE_BITS) * kBins + __umulhi(y, (uint32_t)PPF_N_ANGLE);
-              if (y * (uint32_t)PPF_N_ANGLE - m_lo > m_span) {  // near a bin edge
-                cell = (e[u] >> PPF_ANGLE_BITS) * kBins +
-                       exact_bin<kCheck>(a, (uint32_t)(ep + 32 * u - a.entries), vv);
-                ++my_exact;
-              }
-              if (in_range<kCheck>(a, 7, cell, cells)) atomicAdd(&acc[cell], 1u);
+              const uint32_t y = bsh - (c[u] << kShift);
+              amb |= (y * (uint32_t)PPF_N_ANGLE - m_lo > m_span) ? (1u << u) : 0u;
+              c[u] = (c[u] >> PPF_ANGLE_BITS) * kBins + __umulhi(y, (uint32_t)PPF_N_ANGLE);
             }
+#pragma unroll
+            for (int u = 0; u < kUnroll; ++u)
+              if (in_range<kCheck>(a, 8, c[u], cells)) atomicAdd(&acc[c[u]], 1u);
+            if (amb) fix_up(amb, ep);
           }
           for (uint32_t k = nfull * 32 * kUnroll + lane; k < n_here; k += 32) {
             const uint32_t e = __ldg(a.entries + start + k);
