@@ -293,13 +293,15 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
         const uint32_t n_here = end - start;
         // A vote near a bin edge was counted in its fast cell; move it to the
         // cell of the reference's exact arithmetic (rare: ~1.7e-4 of votes).
-        auto fix_up = [&](uint32_t amb, const uint32_t* first_entry) {
-          for (int u = 0; amb; ++u, amb >>= 1) {
-            if (!(amb & 1u)) continue;
+        auto fix_up = [&](const uint32_t* first_entry) {
+#pragma unroll 1
+          for (int u = 0; u < kUnroll; ++u) {
             const uint32_t pos = (uint32_t)(first_entry + 32 * u - a.entries);
             const uint32_t e = __ldg(a.entries + pos);
+            const uint32_t y = bsh - (e << kShift);
+            if (!(y * (uint32_t)PPF_N_ANGLE - m_lo > m_span)) continue;
             const uint32_t row = (e >> PPF_ANGLE_BITS) * kBins;
-            const uint32_t fast = row + __umulhi(bsh - (e << kShift), (uint32_t)PPF_N_ANGLE);
+            const uint32_t fast = row + __umulhi(y, (uint32_t)PPF_N_ANGLE);
             const uint32_t exact = row + exact_bin<kCheck>(a, pos, vv);
             if (exact != fast && in_range<kCheck>(a, 7, exact, cells)) {
               atomicAdd(&acc[fast], 0xffffffffu);
@@ -323,19 +325,19 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
           const uint32_t nfull = n_here / (32 * kUnroll);
           for (uint32_t it = 0; it < nfull; ++it, ep += 32 * kUnroll) {
             uint32_t c[kUnroll];
-            uint32_t amb = 0;
+            bool amb = false;
 #pragma unroll
             for (int u = 0; u < kUnroll; ++u) c[u] = __ldg(ep + 32 * u);
 #pragma unroll
             for (int u = 0; u < kUnroll; ++u) {
               const uint32_t y = bsh - (c[u] << kShift);
-              amb |= (y * (uint32_t)PPF_N_ANGLE - m_lo > m_span) ? (1u << u) : 0u;
+              amb |= y * (uint32_t)PPF_N_ANGLE - m_lo > m_span;
               c[u] = (c[u] >> PPF_ANGLE_BITS) * kBins + __umulhi(y, (uint32_t)PPF_N_ANGLE);
             }
 #pragma unroll
             for (int u = 0; u < kUnroll; ++u)
               if (in_range<kCheck>(a, 8, c[u], cells)) atomicAdd(&acc[c[u]], 1u);
-            if (amb) fix_up(amb, ep);
+            if (amb) fix_up(ep);
           }
           for (uint32_t k = nfull * 32 * kUnroll + lane; k < n_here; k += 32) {
             const uint32_t e = __ldg(a.entries + start + k);
