@@ -104,6 +104,19 @@ ppf_status ppf_scene_destroy(ppf_scene_t s);
  * with the model's d_dist. */
 ppf_status ppf_model_lookup(ppf_model_t m, ppf_scene_t s, float* pose_out, ppf_stats* stats);
 
+/* n lookups, request i = (models[i], scenes[i]), with one batched vote pass:
+ * the loop of Model::ppf_lookup calls in ppf_registration
+ * (src/cuda/ppf.cu:57-96, src/cuda/model.cu:269-306) over resident models.
+ * All work items of all requests share one persistent launch; the threshold,
+ * poses and clustering then run per request.  Each pose and stats record is
+ * the one ppf_model_lookup gives for the same request.  poses_out: n x 16
+ * (host or device); stats_out: n records or NULL (vote_ms is the batch's
+ * vote time split by work items).  Returns PPF_ERR_NO_VOTES when any request
+ * had no vote above the threshold (its pose is zero).  A model may appear in
+ * several requests; its inspection getters then show its last request. */
+ppf_status ppf_lookup_batch(ppf_context_t ctx, uint64_t n, const ppf_model_t* models,
+                            const ppf_scene_t* scenes, float* poses_out, ppf_stats* stats_out);
+
 /* ppf_registration(scene_clouds, model_clouds, model_d_dists,
  * ref_point_downsample_factor, vote_count_threshold, cpu_clustering,
  * use_l1_norm, use_averaged_clusters, devUse, model_weights)

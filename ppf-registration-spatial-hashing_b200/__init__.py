@@ -16,6 +16,7 @@ from .api import (  # noqa: F401
     PPFError,
     Scene,
     default_context,
+    lookup_batch,
     pair_keys,
     ppf_registration,
 )

@@ -87,6 +87,7 @@ SIGNATURES = {
     "ppf_pair_keys": (C.c_int, [_vp, _vp, _vp, C.c_uint64, C.c_float, C.c_uint32, _vp]),
     "ppf_model_all_votes": (C.c_int, [_vp, _vp, _u64p, _u32p, C.c_uint64, _u64p]),
     "ppf_model_pair_vote_counts": (C.c_int, [_vp, _vp, _vp]),
+    "ppf_lookup_batch": (C.c_int, [_vp, C.c_uint64, _vp, _vp, _vp, _vp]),
     "ppf_model_vote_cells_noalloc": (
         C.c_int,
         [_vp, _vp, _vp, C.c_uint64, C.c_uint32, C.c_float, _vp, _vp, C.c_uint64, _u64p, _u32p],

@@ -319,6 +319,30 @@ def pair_keys(cloud, d_dist: float, ref_point_downsample_factor: int = 1, contex
     return out.reshape(bp.n, bp.n)
 
 
+def lookup_batch(models, scenes, context=None, return_stats: bool = False, raise_on_no_votes: bool = True):
+    """Lookups of (models[i], scenes[i]) with one batched vote pass.
+
+    Each pose equals Model.ppf_lookup(scene) for the same pair; returns an
+    (n, 4, 4) array (and the per-request stats dicts with return_stats).
+    """
+    models, scenes = list(models), list(scenes)
+    if len(models) != len(scenes):
+        raise ValueError("models and scenes must have the same length")
+    ctx = context or (models[0].ctx if models else default_context())
+    n = len(models)
+    mh = (C.c_void_p * max(n, 1))(*[m.handle for m in models])
+    sh = (C.c_void_p * max(n, 1))(*[s.handle for s in scenes])
+    poses = np.zeros((max(n, 1), 16), np.float32)
+    stats = (_capi.ppf_stats * max(n, 1))()
+    status = _lib().ppf_lookup_batch(ctx.handle, n, mh, sh, C.c_void_p(poses.ctypes.data), stats)
+    if not (status == 4 and not raise_on_no_votes):
+        _check(status)
+    out = poses[:n].reshape(n, 4, 4)
+    if return_stats:
+        return out, [stats[i].as_dict() for i in range(n)]
+    return out
+
+
 def ppf_registration(scene_clouds, model_clouds, model_d_dists, ref_point_downsample_factor=1,
                      vote_count_threshold=0.4, cpu_clustering=False, use_l1_norm=False,
                      use_averaged_clusters=False, devUse=0, model_weights=None, context=None,

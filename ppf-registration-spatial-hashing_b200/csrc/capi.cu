@@ -20,6 +20,10 @@ Context::~Context() {
   scratch.release();
   cand_codes.release();
   cand_counts.release();
+  batch_args.release();
+  batch_off.release();
+  batch_counters.release();
+  batch_redo.release();
   redo_items.release();
   sort32.release();
   sort64.release();
@@ -63,14 +67,16 @@ struct LookupOut {
   ppf_stats stats{};
 };
 
-// Model::ppf_lookup + the pose extraction of ppf_registration.
-LookupOut lookup(Model& m, const SceneData& s) {
+// The part of Model::ppf_lookup after the vote pass (threshold, order,
+// poses, clustering) and the pose extraction of ppf_registration, on the
+// candidate cells of one vote pass.  ev[2] marks the lookup's start.
+LookupOut finish_lookup(Model& m, const SceneData& s, const VoteResult& vr,
+                        const unsigned long long* cand_code, const uint32_t* cand_count,
+                        size_t launches0) {
   Context& ctx = *m.ctx;
   LookupState& st = m.last;
   LookupOut out;
-  const size_t launches0 = ctx.launches;
-  PPF_CUDA(cudaEventRecord(ctx.ev[2], ctx.stream));
-  VoteResult vr = run_votes(ctx, m, s, false, -1.f);
+  m.cand_hint = vr.n_cand;
   st.U = 0;
   out.stats.n_votes = vr.n_votes;
   out.stats.n_matched_pairs = vr.n_matched;
@@ -85,7 +91,7 @@ LookupOut lookup(Model& m, const SceneData& s) {
   const float min_votecount = m.vote_count_threshold * (float)vr.max_count;
   out.stats.min_votecount = min_votecount;
   out.stats.n_candidates = vr.n_cand;
-  const size_t U = select_votes(ctx, m, s, st, vr.n_cand, min_votecount);
+  const size_t U = select_votes(ctx, m, s, st, cand_code, cand_count, vr.n_cand, min_votecount);
   out.stats.n_kept = U;
   if (U == 0) {
     out.status = PPF_ERR_NO_VOTES;
@@ -120,6 +126,52 @@ LookupOut lookup(Model& m, const SceneData& s) {
   PPF_REQUIRE(!(flags & kFlagSpinTimeout), PPF_ERR_TIMEOUT, "radix sort look-back timed out");
   PPF_CUDA(cudaEventElapsedTime(&out.stats.total_ms, ctx.ev[2], ctx.ev[3]));
   out.stats.gpu_launches = (uint32_t)(ctx.launches - launches0);
+  return out;
+}
+
+// Model::ppf_lookup + the pose extraction of ppf_registration.
+LookupOut lookup(Model& m, const SceneData& s) {
+  Context& ctx = *m.ctx;
+  const size_t launches0 = ctx.launches;
+  PPF_CUDA(cudaEventRecord(ctx.ev[2], ctx.stream));
+  VoteResult vr = run_votes(ctx, m, s, false, -1.f);
+  return finish_lookup(m, s, vr, ctx.cand_codes.as<unsigned long long>(), ctx.cand_counts.as<uint32_t>(),
+                       launches0);
+}
+
+// Several lookups with one batched vote pass: request i is (models[i],
+// scenes[i]).  Candidate buffers are sized from each model's last pass,
+// within a budget shared by the batch.
+std::vector<LookupOut> lookup_batch(Context& ctx, const std::vector<Model*>& models,
+                                    const std::vector<const SceneData*>& scenes) {
+  const size_t n = models.size();
+  const size_t launches0 = ctx.launches;
+  PPF_CUDA(cudaEventRecord(ctx.ev[2], ctx.stream));
+  std::vector<BatchVote> reqs(n);
+  constexpr size_t kBudgetCells = size_t(1) << 28;  // 3 GB of candidate cells over the batch
+  size_t want = 0;
+  for (size_t i = 0; i < n; ++i) {
+    reqs[i].m = models[i];
+    reqs[i].s = scenes[i];
+    const size_t hint = models[i]->cand_hint;
+    reqs[i].cap = hint ? hint + hint / 4 + 65536 : (size_t(1) << 22);
+    want += reqs[i].cap;
+  }
+  if (want > kBudgetCells)
+    for (auto& r : reqs) r.cap = std::max<size_t>(r.cap * (double)kBudgetCells / (double)want, 65536);
+  // test hook: a small capacity exercises the per-request growth path
+  if (const char* e = std::getenv("PPF_B200_BATCH_CAP")) {
+    const long long v = std::atoll(e);
+    if (v > 0)
+      for (auto& r : reqs) r.cap = (size_t)v;
+  }
+  run_votes_batch(ctx, reqs);
+  std::vector<LookupOut> out(n);
+  for (size_t i = 0; i < n; ++i) {
+    out[i] = finish_lookup(*models[i], *scenes[i], reqs[i].r, reqs[i].codes.as<unsigned long long>(),
+                           reqs[i].counts.as<uint32_t>(), i == 0 ? launches0 : ctx.launches);
+    PPF_CUDA(cudaEventRecord(ctx.ev[2], ctx.stream));
+  }
   return out;
 }
 
@@ -293,6 +345,37 @@ ppf_status ppf_model_lookup(ppf_model_t m, ppf_scene_t s, float* pose_out, ppf_s
     PPF_CUDA(cudaMemcpy(pose_out, r.pose, sizeof(r.pose), cudaMemcpyDefault));
     if (stats) *stats = r.stats;
     if (r.status != PPF_OK) return fail(r.status, "no vote passed the threshold");
+    return PPF_OK;
+  });
+}
+
+ppf_status ppf_lookup_batch(ppf_context_t ctx, uint64_t n, const ppf_model_t* models,
+                            const ppf_scene_t* scenes, float* poses_out, ppf_stats* stats_out) {
+  return guarded([&]() {
+    PPF_REQUIRE(ctx, PPF_ERR_INVALID_ARGUMENT, "null context");
+    if (n == 0) return PPF_OK;
+    PPF_REQUIRE(models && scenes && poses_out, PPF_ERR_INVALID_ARGUMENT, "null models, scenes or poses");
+    std::vector<Model*> ms(n);
+    std::vector<const SceneData*> ss(n);
+    for (uint64_t i = 0; i < n; ++i) {
+      PPF_REQUIRE(models[i] && scenes[i], PPF_ERR_INVALID_ARGUMENT, "null model or scene in the batch");
+      PPF_REQUIRE(models[i]->m.ctx == &ctx->c && scenes[i]->ctx == &ctx->c, PPF_ERR_INVALID_ARGUMENT,
+                  "batch model or scene on another context");
+      ms[i] = &models[i]->m;
+      ss[i] = &scenes[i]->s;
+    }
+    PPF_CUDA(cudaSetDevice(ctx->c.device));
+    StreamScope scope(ctx->c.stream);
+    std::vector<LookupOut> r = lookup_batch(ctx->c, ms, ss);
+    std::vector<float> poses(n * 16);
+    ppf_status worst = PPF_OK;
+    for (uint64_t i = 0; i < n; ++i) {
+      std::memcpy(&poses[16 * i], r[i].pose, sizeof(r[i].pose));
+      if (stats_out) stats_out[i] = r[i].stats;
+      if (r[i].status != PPF_OK) worst = r[i].status;
+    }
+    PPF_CUDA(cudaMemcpy(poses_out, poses.data(), poses.size() * sizeof(float), cudaMemcpyDefault));
+    if (worst != PPF_OK) return fail(worst, "no vote passed the threshold for at least one request");
     return PPF_OK;
   });
 }

@@ -38,6 +38,7 @@ struct Context {
   DevBuf scratch;    // run-table scratch
   // vote-pass candidate cells (code, count), kept and grown across lookups
   DevBuf cand_codes, cand_counts, redo_items;
+  DevBuf batch_args, batch_off, batch_counters, batch_redo;  // batched vote pass
   size_t cand_cap = size_t(1) << 24;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   int vote_smem_limit = 0;  // max dynamic shared memory per vote block
@@ -108,6 +109,7 @@ struct Model {
   ModelTables t;
   float vote_count_threshold = 0.4f;
   bool cpu_clustering = false, use_l1_norm = false, use_averaged_clusters = false;
+  size_t cand_hint = 0;  // candidate cells of the last vote pass (sizes batch buffers)
   LookupState last;
 };
 
@@ -133,6 +135,18 @@ struct VoteResult {
 // floor >= 0 forces the emission floor.  Candidates land in
 // ctx.cand_codes / ctx.cand_counts.
 VoteResult run_votes(Context& ctx, const Model& m, const SceneData& s, bool emit_all, float floor);
+// One request of a batched vote pass: its candidate cells land in its own
+// buffers (cap cells, grown if they do not fit).
+struct BatchVote {
+  const Model* m = nullptr;
+  const SceneData* s = nullptr;
+  size_t cap = 0;
+  DevBuf codes, counts;
+  VoteResult r;
+};
+// The vote passes of all requests in one persistent launch (threshold x
+// running maximum emission, as run_votes with emit_all = false).
+void run_votes_batch(Context& ctx, std::vector<BatchVote>& reqs);
 void pair_vote_counts(Context& ctx, const Model& m, const SceneData& s, uint64_t* out_dev);
 // The vote pass with no device allocation: scene and outputs are the
 // caller's device arrays, everything else lives in a static device array of
@@ -145,7 +159,8 @@ void vote_cells_noalloc(Context& ctx, const Model& m, const float* xyz, const fl
 // Filters the candidates to the kept votes and orders them (count desc,
 // code asc); returns U.
 size_t select_votes(Context& ctx, const Model& m, const SceneData& s, LookupState& st,
-                    size_t n_cand, float min_votecount);
+                    const unsigned long long* cand_code, const uint32_t* cand_count, size_t n_cand,
+                    float min_votecount);
 // Orders arbitrary (code, count) pairs by code ascending (all-votes dump).
 void sort_by_code(Context& ctx, LookupState& st, size_t n);
 void compute_poses(Context& ctx, const Model& m, const SceneData& s, LookupState& st);

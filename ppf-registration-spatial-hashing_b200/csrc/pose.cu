@@ -457,13 +457,14 @@ T* grow(DevBuf& b, size_t n) {
 }  // namespace
 
 size_t select_votes(Context& ctx, const Model& m, const SceneData& s, LookupState& st,
-                    size_t n_cand, float min_votecount) {
+                    const unsigned long long* cand_code, const uint32_t* cand_count, size_t n_cand,
+                    float min_votecount) {
   cudaStream_t stream = ctx.stream;
   unsigned long long* fcode = grow<unsigned long long>(st.tmp64, n_cand + 1);
   uint32_t* fcount = grow<uint32_t>(st.tmp32a, n_cand + 1);
   PPF_CUDA(cudaMemsetAsync(ctx.counters.ptr, 0, 4, stream));
   filter_kernel<<<grid_for(n_cand, 256), 256, 0, stream>>>(
-      ctx.cand_codes.as<unsigned long long>(), ctx.cand_counts.as<uint32_t>(), n_cand, min_votecount,
+      cand_code, cand_count, n_cand, min_votecount,
       fcode, fcount, ctx.counters.as<uint32_t>());
   PPF_CUDA(cudaGetLastError());
   ctx.launches++;

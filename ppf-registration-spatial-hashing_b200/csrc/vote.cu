@@ -157,8 +157,52 @@ __device__ __forceinline__ uint32_t exact_bin(const VoteArgs& a, uint32_t pos, f
   return alpha_bin_exact(u, v);
 }
 
+// Per-block shared state of a vote kernel besides the dynamic queue and
+// accumulator.
+struct VoteShared {
+  uint32_t item, next, max, base;
+  uint32_t scan_seg[kVoteWarps];   // scratch of the per-tile segment scan
+  uint32_t scan_emit[kVoteWarps];  // scratch of the emission scan
+  uint32_t wmax[kVoteWarps];       // per-warp maxima of the accumulator
+};
+
+// Per-thread vote statistics, folded into a request's counters when the
+// block leaves the request.
+struct VoteStats {
+  unsigned long long votes = 0, matched = 0, exact = 0;
+};
+
+__device__ __forceinline__ void flush_stats(const VoteArgs& a, VoteStats& st) {
+  for (int o = 16; o; o >>= 1) {
+    st.votes += __shfl_xor_sync(0xffffffffu, st.votes, o);
+    st.matched += __shfl_xor_sync(0xffffffffu, st.matched, o);
+    st.exact += __shfl_xor_sync(0xffffffffu, st.exact, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (st.votes) atomicAdd(&a.stats[0], st.votes);
+    if (st.matched) atomicAdd(&a.stats[1], st.matched);
+    if (st.exact) atomicAdd(&a.stats[2], st.exact);
+  }
+  st = VoteStats();
+}
+
+// Fetches the next work item into sh.item (one atomic per block).
+__device__ __forceinline__ uint32_t fetch_item(uint32_t* work_counter, VoteShared& sh) {
+  if ((threadIdx.x >> 5) == 0) {
+    uint32_t next = 0;
+    if ((threadIdx.x & 31) == 0) next = atomicAdd(work_counter, 1u);
+    next = __shfl_sync(0xffffffffu, next, 0);
+    if ((threadIdx.x & 31) == 0) sh.item = next;
+  }
+  block_sync();
+  return sh.item;
+}
+
+// One work item (s_r, chunk) of request `a`: slot_of_item indexes a's items
+// (or a.item_list).  Called by every thread of the block.
 template <bool kCheck>
-__global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
+__device__ __forceinline__ void vote_item(const VoteArgs& a, uint32_t slot_of_item, VoteShared& sh,
+                                          VoteStats& st) {
   extern __shared__ __align__(16) uint32_t smem[];
   uint32_t* q_lo = smem;                        // [kVoteThreads]
   uint32_t* q_len = q_lo + kVoteThreads;        // [kVoteThreads]
@@ -167,25 +211,9 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
   uint32_t* q_seg = reinterpret_cast<uint32_t*>(q_v + kVoteThreads);    // [kVoteThreads + 4]
   uint32_t* acc = q_seg + kVoteThreads + 4;
 
-  __shared__ uint32_t s_item, s_next, s_max, s_base;
-  __shared__ uint32_t s_scan_seg[kVoteWarps];   // scratch of the per-tile segment scan
-  __shared__ uint32_t s_scan_emit[kVoteWarps];  // scratch of the emission scan
-  __shared__ uint32_t s_wmax[kVoteWarps];       // per-warp maxima of the accumulator
-
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t cells = a.chunk * kBins;
-  unsigned long long my_votes = 0, my_matched = 0, my_exact = 0;
-
-  for (;;) {
-    if (warp == 0) {
-      uint32_t next = 0;
-      if (lane == 0) next = atomicAdd(a.work_counter, 1u);
-      next = __shfl_sync(0xffffffffu, next, 0);
-      if (lane == 0) s_item = next;
-    }
-    block_sync();
-    const uint32_t slot_of_item = s_item;
-    if (slot_of_item >= a.n_items) break;
+  {
     const uint32_t item = a.item_list ? a.item_list[slot_of_item] : slot_of_item;
     const uint32_t c = item % a.n_chunks;
     // ref < n_ref, so sr = ref * ref_df < n_s
@@ -219,8 +247,8 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
             len = __ldg(sp + c + 1) - lo;
             if (kCheck && !in_range<kCheck>(a, 3, (unsigned long long)lo + len, a.P + 1)) len = 0;
             if (c == 0 && !a.item_list) {
-              my_votes += __ldg(a.run_count + run);
-              my_matched += 1;
+              st.votes += __ldg(a.run_count + run);
+              st.matched += 1;
             }
             if (len) {
               v = frame_point_yz(fs, pi);
@@ -231,7 +259,7 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
         }
       }
       uint32_t n_seg_total;
-      const uint32_t seg0 = block_excl_scan((len + kSeg - 1) / kSeg, s_scan_seg, n_seg_total);
+      const uint32_t seg0 = block_excl_scan((len + kSeg - 1) / kSeg, sh.scan_seg, n_seg_total);
       q_lo[tid] = lo;
       q_len[tid] = len;
       q_beta[tid] = beta;
@@ -239,7 +267,7 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
       q_seg[tid] = seg0;
       if (tid == 0) {
         q_seg[kVoteThreads] = n_seg_total;
-        s_next = kVoteWarps;
+        sh.next = kVoteWarps;
       }
       block_sync();
       if (kCheck) {
@@ -307,7 +335,7 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
               atomicAdd(&acc[fast], 0xffffffffu);
               atomicAdd(&acc[exact], 1u);
             }
-            ++my_exact;
+            ++st.exact;
           }
         };
         if (bw & kExactOnly) {
@@ -316,7 +344,7 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
             const uint32_t row = (__ldg(a.entries + start + k) >> PPF_ANGLE_BITS) * kBins;
             const uint32_t cell = row + exact_bin<kCheck>(a, start + k, vv);
             if (in_range<kCheck>(a, 6, cell, cells)) atomicAdd(&acc[cell], 1u);
-            ++my_exact;
+            ++st.exact;
           }
         } else {
           // kUnroll entries per lane per pass, branch-free: the fast cell of
@@ -345,12 +373,12 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
             uint32_t cell = (e >> PPF_ANGLE_BITS) * kBins + __umulhi(y, (uint32_t)PPF_N_ANGLE);
             if (y * (uint32_t)PPF_N_ANGLE - m_lo > m_span) {
               cell = (e >> PPF_ANGLE_BITS) * kBins + exact_bin<kCheck>(a, start + k, vv);
-              ++my_exact;
+              ++st.exact;
             }
             if (in_range<kCheck>(a, 8, cell, cells)) atomicAdd(&acc[cell], 1u);
           }
         }
-        if (lane == 0) s = atomicAdd(&s_next, 1u);
+        if (lane == 0) s = atomicAdd(&sh.next, 1u);
         s = __shfl_sync(0xffffffffu, s, 0);
       }
       if (kCheck && (q_seg[tid] != seg0 || q_len[tid] != len || q_lo[tid] != lo))
@@ -366,19 +394,19 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
     for (uint32_t w = tid; w < cells; w += kVoteThreads) lmax = max(lmax, acc[w]);
 #pragma unroll
     for (int o = 16; o; o >>= 1) lmax = max(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
-    if (lane == 0) s_wmax[warp] = lmax;
+    if (lane == 0) sh.wmax[warp] = lmax;
     block_sync();
     if (warp == 0) {
-      uint32_t m = s_wmax[lane];
+      uint32_t m = sh.wmax[lane];
 #pragma unroll
       for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
       uint32_t old = 0;
       if (lane == 0) old = atomicMax(a.global_max, m);
       old = __shfl_sync(0xffffffffu, old, 0);
-      if (lane == 0) s_max = max(old, m);
+      if (lane == 0) sh.max = max(old, m);
     }
     block_sync();
-    const float floor_v = a.floor >= 0.f ? a.floor : a.thr * (float)s_max;
+    const float floor_v = a.floor >= 0.f ? a.floor : a.thr * (float)sh.max;
     // All-or-nothing slot reservation for the item's cells: an item that does
     // not fit writes nothing and is queued for a second launch after the
     // buffer has grown, so the buffer never holds a partial item.
@@ -388,7 +416,7 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
       my_n += (cnt != 0u && (a.emit_all || (float)cnt > floor_v)) ? 1u : 0u;
     }
     uint32_t item_total;
-    const uint32_t my_off = block_excl_scan(my_n, s_scan_emit, item_total);
+    const uint32_t my_off = block_excl_scan(my_n, sh.scan_emit, item_total);
     if (warp == 0) {
       // The whole warp walks the reservation loop in lockstep (lane 0 issues
       // the atomics, every exit condition is warp-uniform).
@@ -414,10 +442,10 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
           if (in_range<kCheck>(a, 9, k, a.n_items_total)) a.redo_items[k] = item;
         }
       }
-      if (lane == 0) s_base = base_slot;
+      if (lane == 0) sh.base = base_slot;
     }
     block_sync();
-    const uint32_t item_base = s_base;
+    const uint32_t item_base = sh.base;
     if (item_base != 0xffffffffu) {
       uint32_t slot = item_base + my_off;
       for (uint32_t cell = tid; cell < cells; cell += kVoteThreads) {
@@ -432,21 +460,64 @@ __global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
         }
       }
     }
-    // The item-fetch barrier at the top of the loop separates these reads of
-    // the accumulator from the next item's clear.
+    // The item-fetch barrier of the caller separates these reads of the
+    // accumulator from the next item's clear.
   }
+}
 
-  // per-block statistics
-  for (int o = 16; o; o >>= 1) {
-    my_votes += __shfl_xor_sync(0xffffffffu, my_votes, o);
-    my_matched += __shfl_xor_sync(0xffffffffu, my_matched, o);
-    my_exact += __shfl_xor_sync(0xffffffffu, my_exact, o);
+template <bool kCheck>
+__global__ void __launch_bounds__(kVoteThreads, 1) vote_kernel(VoteArgs a) {
+  __shared__ VoteShared sh;
+  VoteStats st;
+  for (;;) {
+    const uint32_t slot = fetch_item(a.work_counter, sh);
+    if (slot >= a.n_items) break;
+    vote_item<kCheck>(a, slot, sh, st);
   }
-  if (lane == 0) {
-    if (my_votes) atomicAdd(&a.stats[0], my_votes);
-    if (my_matched) atomicAdd(&a.stats[1], my_matched);
-    if (my_exact) atomicAdd(&a.stats[2], my_exact);
+  flush_stats(a, st);
+}
+
+// Several requests (model, scene) in one persistent launch: work items of
+// all requests are numbered consecutively (request r owns items
+// [item_off[r], item_off[r+1])) and fetched from one counter.  A block copies
+// the arguments of an item's request into shared memory when the request
+// changes; each request keeps its own running maximum, counters, candidate
+// region and list of items that did not fit.
+struct BatchArgs {
+  const VoteArgs* reqs;
+  const uint32_t* item_off;  // n_reqs + 1
+  uint32_t n_reqs, n_items;
+  uint32_t* work_counter;
+};
+
+template <bool kCheck>
+__global__ void __launch_bounds__(kVoteThreads, 1) vote_batch_kernel(BatchArgs b) {
+  __shared__ VoteShared sh;
+  __shared__ VoteArgs s_args;
+  VoteStats st;
+  uint32_t cur = 0xffffffffu;
+  for (;;) {
+    const uint32_t g = fetch_item(b.work_counter, sh);
+    if (g >= b.n_items) break;
+    uint32_t lo = 0, hi = b.n_reqs;  // request r with item_off[r] <= g < item_off[r + 1]
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (__ldg(b.item_off + mid) <= g) lo = mid;
+      else hi = mid;
+    }
+    if (lo != cur) {  // uniform: every thread found the same request
+      if (cur != 0xffffffffu) flush_stats(s_args, st);
+      block_sync();
+      constexpr int kWords = sizeof(VoteArgs) / 4;
+      static_assert(sizeof(VoteArgs) % 4 == 0 && kWords <= kVoteThreads, "request arguments fit one copy pass");
+      if (threadIdx.x < kWords)
+        reinterpret_cast<uint32_t*>(&s_args)[threadIdx.x] = reinterpret_cast<const uint32_t*>(b.reqs + lo)[threadIdx.x];
+      block_sync();
+      cur = lo;
+    }
+    vote_item<kCheck>(s_args, g - __ldg(b.item_off + lo), sh, st);
   }
+  if (cur != 0xffffffffu) flush_stats(s_args, st);
 }
 
 // counts[r * n_s + i]: model run length of a matching scene pair (r, i).
@@ -623,6 +694,145 @@ VoteResult run_votes(Context& ctx, const Model& m, const SceneData& s, bool emit
   r.n_matched = s64[1];
   r.n_exact = s64[2];
   return r;
+}
+
+void run_votes_batch(Context& ctx, std::vector<BatchVote>& reqs) {
+  cudaStream_t stream = ctx.stream;
+  const size_t n = reqs.size();
+  if (n == 0) return;
+  PPF_REQUIRE(n < (1u << 24), PPF_ERR_INVALID_ARGUMENT, "too many requests in one batch");
+  std::vector<VoteArgs> args(n);
+  std::vector<uint32_t> item_off(n + 1, 0);
+  // per request 16 counter words ([1] max, [2] n_cand, [3] n_redo, [4..9]
+  // stats, [10..11] n_needed, [12] work counter of its redo launch), then the
+  // batch's own work counter
+  ctx.batch_counters.reserve((n + 1) * 64);
+  PPF_CUDA(cudaMemsetAsync(ctx.batch_counters.ptr, 0, (n + 1) * 64, stream));
+  PPF_CUDA(cudaMemsetAsync(ctx.flags.ptr, 0, 32 + 80, stream));
+  uint32_t* cnt0 = ctx.batch_counters.as<uint32_t>();
+  size_t total = 0, smem = kVoteQueueBytes;
+  for (size_t i = 0; i < n; ++i) {
+    const VoteArgs a0 = make_args(*reqs[i].m, *reqs[i].s);
+    const uint64_t items = reqs[i].s->n < 2 ? 0 : (uint64_t)a0.n_ref * a0.n_chunks;
+    total += items;
+    PPF_REQUIRE(total < 0xffffffffull, PPF_ERR_INVALID_ARGUMENT, "more than 2^32 work items in one batch");
+    item_off[i + 1] = (uint32_t)total;
+    smem = std::max(smem, kVoteQueueBytes + vote_acc_words(a0.chunk) * 4);
+  }
+  PPF_REQUIRE((int)smem <= ctx.vote_smem_limit, PPF_ERR_INTERNAL, "vote accumulator too large");
+  ctx.batch_redo.reserve(std::max<size_t>(total, 1) * sizeof(uint32_t));
+  for (size_t i = 0; i < n; ++i) {
+    VoteArgs& a = args[i];
+    a = make_args(*reqs[i].m, *reqs[i].s);
+    a.emit_all = 0;
+    a.floor = -1.f;
+    uint32_t* cnt = cnt0 + 16 * i;
+    a.work_counter = nullptr;
+    a.global_max = cnt + 1;
+    a.n_cand = cnt + 2;
+    a.n_redo = cnt + 3;
+    a.stats = reinterpret_cast<unsigned long long*>(cnt + 4);
+    a.n_needed = reinterpret_cast<unsigned long long*>(cnt + 10);
+    a.flags = ctx.flags.as<uint32_t>();
+    a.bad = reinterpret_cast<unsigned long long*>(ctx.flags.as<uint32_t>() + 8);
+    reqs[i].cap = std::max<size_t>(reqs[i].cap, 1024);
+    PPF_REQUIRE(reqs[i].cap < 0xffffffffull, PPF_ERR_INVALID_ARGUMENT, "candidate capacity beyond 2^32");
+    reqs[i].codes.reserve(reqs[i].cap * sizeof(unsigned long long));
+    reqs[i].counts.reserve(reqs[i].cap * sizeof(uint32_t));
+    a.cand_code = reqs[i].codes.as<unsigned long long>();
+    a.cand_count = reqs[i].counts.as<uint32_t>();
+    a.cand_cap = (uint32_t)reqs[i].cap;
+    a.redo_items = ctx.batch_redo.as<uint32_t>() + item_off[i];
+    a.item_list = nullptr;
+    a.n_items = item_off[i + 1] - item_off[i];
+    a.n_items_total = a.n_items;
+  }
+  ctx.batch_args.reserve(n * sizeof(VoteArgs));
+  ctx.batch_off.reserve((n + 1) * sizeof(uint32_t));
+  PPF_CUDA(cudaMemcpyAsync(ctx.batch_args.ptr, args.data(), n * sizeof(VoteArgs), cudaMemcpyHostToDevice, stream));
+  PPF_CUDA(cudaMemcpyAsync(ctx.batch_off.ptr, item_off.data(), (n + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                           stream));
+  BatchArgs b;
+  b.reqs = ctx.batch_args.as<VoteArgs>();
+  b.item_off = ctx.batch_off.as<uint32_t>();
+  b.n_reqs = (uint32_t)n;
+  b.n_items = (uint32_t)total;
+  b.work_counter = cnt0 + 16 * n;
+  const bool check = ctx.checks;
+  auto bkernel = check ? vote_batch_kernel<true> : vote_batch_kernel<false>;
+  auto kernel = check ? vote_kernel<true> : vote_kernel<false>;
+  PPF_CUDA(cudaEventRecord(ctx.ev[0], stream));
+  if (total) {
+    PPF_CUDA(cudaFuncSetAttribute(bkernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    bkernel<<<(unsigned)std::min<size_t>(total, (size_t)sm_count()), kVoteThreads, smem, stream>>>(b);
+    PPF_CUDA(cudaGetLastError());
+    ctx.launches++;
+  }
+  std::vector<uint32_t> h((n + 1) * 16);
+  PPF_CUDA(cudaMemcpyAsync(h.data(), cnt0, (n + 1) * 64, cudaMemcpyDeviceToHost, stream));
+  PPF_CUDA(cudaStreamSynchronize(stream));
+  // Requests whose cells did not all fit: grow their buffers (keeping what was
+  // emitted) and count their remaining items again, one request at a time.
+  for (size_t i = 0; i < n; ++i) {
+    uint32_t* hc = h.data() + 16 * i;
+    reqs[i].r.n_redo = hc[3];
+    if (!hc[3]) continue;
+    unsigned long long needed;
+    memcpy(&needed, hc + 10, sizeof(needed));
+    const size_t want = std::max<size_t>(needed, 2 * reqs[i].cap);
+    PPF_REQUIRE(want < 0xffffffffull, PPF_ERR_OUT_OF_MEMORY, "more than 2^32 vote candidates");
+    DevBuf nc, nn, items;
+    nc.reserve(want * sizeof(unsigned long long));
+    nn.reserve(want * sizeof(uint32_t));
+    items.reserve((size_t)hc[3] * sizeof(uint32_t));
+    PPF_CUDA(cudaMemcpyAsync(nc.ptr, reqs[i].codes.ptr, (size_t)hc[2] * 8, cudaMemcpyDeviceToDevice, stream));
+    PPF_CUDA(cudaMemcpyAsync(nn.ptr, reqs[i].counts.ptr, (size_t)hc[2] * 4, cudaMemcpyDeviceToDevice, stream));
+    PPF_CUDA(cudaMemcpyAsync(items.ptr, args[i].redo_items, (size_t)hc[3] * 4, cudaMemcpyDeviceToDevice, stream));
+    reqs[i].codes = std::move(nc);
+    reqs[i].counts = std::move(nn);
+    reqs[i].cap = want;
+    VoteArgs a = args[i];
+    a.cand_code = reqs[i].codes.as<unsigned long long>();
+    a.cand_count = reqs[i].counts.as<uint32_t>();
+    a.cand_cap = (uint32_t)want;
+    a.item_list = items.as<uint32_t>();
+    a.n_items = hc[3];
+    a.work_counter = cnt0 + 16 * i + 12;
+    PPF_CUDA(cudaMemsetAsync(a.n_redo, 0, 4, stream));
+    const size_t smem_i = kVoteQueueBytes + vote_acc_words(a.chunk) * 4;
+    PPF_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_i));
+    kernel<<<(unsigned)std::min<size_t>(a.n_items, (size_t)sm_count()), kVoteThreads, smem_i, stream>>>(a);
+    PPF_CUDA(cudaGetLastError());
+    ctx.launches++;
+    PPF_CUDA(cudaMemcpyAsync(hc, cnt0 + 16 * i, 64, cudaMemcpyDeviceToHost, stream));
+    PPF_CUDA(cudaStreamSynchronize(stream));
+    PPF_REQUIRE(hc[3] == 0, PPF_ERR_INTERNAL, "vote candidates still do not fit");
+  }
+  PPF_CUDA(cudaEventRecord(ctx.ev[1], stream));
+  PPF_CUDA(cudaEventSynchronize(ctx.ev[1]));
+  {
+    unsigned long long rec[14];
+    PPF_CUDA(cudaMemcpyAsync(rec, ctx.flags.ptr, sizeof(rec), cudaMemcpyDeviceToHost, stream));
+    PPF_CUDA(cudaStreamSynchronize(stream));
+    if ((uint32_t)(rec[0] & 0xffffffffu) & kFlagBadIndex)
+      throw Error(PPF_ERR_INTERNAL, "vote kernel index out of range: site " + std::to_string(rec[4]) +
+                                        " value " + std::to_string(rec[5]) + " bound " + std::to_string(rec[6]));
+  }
+  float ms = 0;
+  PPF_CUDA(cudaEventElapsedTime(&ms, ctx.ev[0], ctx.ev[1]));
+  for (size_t i = 0; i < n; ++i) {
+    const uint32_t* hc = h.data() + 16 * i;
+    VoteResult& r = reqs[i].r;
+    r.max_count = hc[1];
+    r.n_cand = hc[2];
+    unsigned long long s64[3];
+    memcpy(s64, hc + 4, sizeof(s64));
+    r.n_votes = s64[0];
+    r.n_matched = s64[1];
+    r.n_exact = s64[2];
+    // the batch's device time, split by work items
+    r.vote_ms = total ? ms * (float)(item_off[i + 1] - item_off[i]) / (float)total : 0.f;
+  }
 }
 
 void pair_vote_counts(Context& ctx, const Model& m, const SceneData& s, uint64_t* out_dev) {
