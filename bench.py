@@ -12,6 +12,9 @@ value : registrations/s with the clouds already in device memory
 e2e   : the same through the C ABI with host buffers in pinned memory; the
         host->device copies of the clouds and the device->host read of the
         poses are inside the timed region.
+clocks: nvidia-smi samples the SM clock and throttle reasons every 2.5 s inside
+        the timed region (denser sampling stretched the host-synchronised part
+        of a step by up to 10% on B200).
 L2    : a 256 MB buffer is written on the engine's stream after every timed
         step (inside the timed region), and each step's model tables (about
         1 GB for the four models) exceed the 126 MB L2 anyway.
@@ -91,8 +94,9 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, interval_ms=2500):
         self.gpu = gpu_index
+        self.interval_ms = int(interval_ms)
         self.proc = None
         self.path = ROOT / "gpurun_out" / f"clocks_rank{gpu_index}.csv"
 
@@ -102,7 +106,7 @@ class ClockSampler:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                 "-lms", str(self.interval_ms)], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
         return self
@@ -221,6 +225,9 @@ def main():
     ap.add_argument("--cpu-refs", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--clock-interval-ms", type=int, default=2500,
+                    help="nvidia-smi sampling interval during the timed region (each query stalls the "
+                         "engine's CUDA calls briefly)")
     ap.add_argument("--profile-case", action="store_true",
                     help="one lookup of model 0 at ref_point_df=50 (short vote launch for ncu)")
     args = ap.parse_args()
@@ -271,7 +278,7 @@ def main():
     vote_ms = 0.0
     votes = 0
     pairs = 0
-    with ClockSampler(local) as clk:
+    with ClockSampler(local, args.clock_interval_ms) as clk:
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         ev0.record(stream)

@@ -67,6 +67,13 @@ struct LookupOut {
   ppf_stats stats{};
 };
 
+uint64_t model_signature(const Model& m) {
+  uint32_t d, t;
+  std::memcpy(&d, &m.t.d_dist, 4);
+  std::memcpy(&t, &m.vote_count_threshold, 4);
+  return ((uint64_t)m.t.n * 0x9E3779B97F4A7C15ull) ^ ((uint64_t)d << 21) ^ ((uint64_t)t * 0xC2B2AE3Dull);
+}
+
 // The part of Model::ppf_lookup after the vote pass (threshold, order,
 // poses, clustering) and the pose extraction of ppf_registration, on the
 // candidate cells of one vote pass.  ev[2] marks the lookup's start.
@@ -77,6 +84,7 @@ LookupOut finish_lookup(Model& m, const SceneData& s, const VoteResult& vr,
   LookupState& st = m.last;
   LookupOut out;
   m.cand_hint = vr.n_cand;
+  ctx.cand_hints[model_signature(m)] = vr.n_cand;
   st.U = 0;
   out.stats.n_votes = vr.n_votes;
   out.stats.n_matched_pairs = vr.n_matched;
@@ -153,7 +161,11 @@ std::vector<LookupOut> lookup_batch(Context& ctx, const std::vector<Model*>& mod
   for (size_t i = 0; i < n; ++i) {
     reqs[i].m = models[i];
     reqs[i].s = scenes[i];
-    const size_t hint = models[i]->cand_hint;
+    size_t hint = models[i]->cand_hint;
+    if (!hint) {
+      auto it = ctx.cand_hints.find(model_signature(*models[i]));
+      if (it != ctx.cand_hints.end()) hint = it->second;
+    }
     reqs[i].cap = hint ? hint + hint / 4 + 65536 : (size_t(1) << 22);
     want += reqs[i].cap;
   }
@@ -406,24 +418,49 @@ ppf_status ppf_registration(ppf_context_t ctx, uint64_t n_scenes, const float* c
     StreamScope scope(c->c.stream);
     std::vector<float> host_poses(n_scenes * n_models * 16, 0.f);
     ppf_status worst = PPF_OK;
-    for (uint64_t j = 0; j < n_models; ++j) {
-      ppf_model_t m = nullptr;
-      ppf_status st = ppf_model_create(c, model_xyz[j], model_nxyz[j], model_n[j], model_d_dists[j],
-                                       vote_count_threshold, cpu_clustering, use_l1_norm,
-                                       use_averaged_clusters, &m);
-      if (st != PPF_OK) throw Error(st, g_last_error);
-      std::unique_ptr<ppf_model_s, ppf_status (*)(ppf_model_t)> mg(m, ppf_model_destroy);
-      for (uint64_t i = 0; i < n_scenes; ++i) {
-        ppf_scene_t s = nullptr;
-        st = ppf_scene_create(c, scene_xyz[i], scene_nxyz[i], scene_n[i], model_d_dists[j],
-                              ref_point_df, &s);
+    using ModelPtr = std::unique_ptr<ppf_model_s, ppf_status (*)(ppf_model_t)>;
+    using ScenePtr = std::unique_ptr<ppf_scene_s, ppf_status (*)(ppf_scene_t)>;
+    // The reference builds each model again for every scene; a model built
+    // once gives the same results.  Models are built in groups whose tables
+    // (about 17 bytes per ordered pair) fit a device budget, and all (scene,
+    // model) pairs of a group share one batched vote pass.
+    constexpr double kGroupBytes = 48e9;
+    for (uint64_t j0 = 0; j0 < n_models;) {
+      uint64_t j1 = j0;
+      double bytes = 0;
+      while (j1 < n_models && (j1 == j0 || bytes + 17.0 * model_n[j1] * model_n[j1] <= kGroupBytes))
+        bytes += 17.0 * model_n[j1] * model_n[j1], ++j1;
+      std::vector<ModelPtr> models;
+      for (uint64_t j = j0; j < j1; ++j) {
+        ppf_model_t m = nullptr;
+        ppf_status st = ppf_model_create(c, model_xyz[j], model_nxyz[j], model_n[j], model_d_dists[j],
+                                         vote_count_threshold, cpu_clustering, use_l1_norm,
+                                         use_averaged_clusters, &m);
         if (st != PPF_OK) throw Error(st, g_last_error);
-        std::unique_ptr<ppf_scene_s, ppf_status (*)(ppf_scene_t)> sg(s, ppf_scene_destroy);
-        LookupOut r = lookup(m->m, s->s);
-        std::memcpy(&host_poses[(i * n_models + j) * 16], r.pose, sizeof(r.pose));
-        if (stats_out) stats_out[i * n_models + j] = r.stats;
-        if (r.status != PPF_OK) worst = r.status;
+        models.emplace_back(m, ppf_model_destroy);
       }
+      std::vector<ScenePtr> scenes;
+      std::vector<Model*> ms;
+      std::vector<const SceneData*> ss;
+      std::vector<size_t> slot;
+      for (uint64_t i = 0; i < n_scenes; ++i)
+        for (uint64_t j = j0; j < j1; ++j) {
+          ppf_scene_t s = nullptr;
+          ppf_status st = ppf_scene_create(c, scene_xyz[i], scene_nxyz[i], scene_n[i], model_d_dists[j],
+                                           ref_point_df, &s);
+          if (st != PPF_OK) throw Error(st, g_last_error);
+          scenes.emplace_back(s, ppf_scene_destroy);
+          ms.push_back(&models[j - j0]->m);
+          ss.push_back(&s->s);
+          slot.push_back(i * n_models + j);
+        }
+      std::vector<LookupOut> r = lookup_batch(c->c, ms, ss);
+      for (size_t k = 0; k < r.size(); ++k) {
+        std::memcpy(&host_poses[slot[k] * 16], r[k].pose, sizeof(r[k].pose));
+        if (stats_out) stats_out[slot[k]] = r[k].stats;
+        if (r[k].status != PPF_OK) worst = r[k].status;
+      }
+      j0 = j1;
     }
     if (!host_poses.empty())
       PPF_CUDA(cudaMemcpy(poses_out, host_poses.data(), host_poses.size() * sizeof(float),

@@ -2,6 +2,7 @@
 // resident scenes, and the device-side layout the kernels consume.
 #pragma once
 
+#include <unordered_map>
 #include <vector>
 
 #include "common.cuh"
@@ -39,6 +40,10 @@ struct Context {
   // vote-pass candidate cells (code, count), kept and grown across lookups
   DevBuf cand_codes, cand_counts, redo_items;
   DevBuf batch_args, batch_off, batch_counters, batch_redo;  // batched vote pass
+  // candidate cells the last vote pass of a model with this signature
+  // (points, d_dist, threshold) emitted; sizes the next batch's buffers when
+  // the same model is built again
+  std::unordered_map<uint64_t, size_t> cand_hints;
   size_t cand_cap = size_t(1) << 24;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   int vote_smem_limit = 0;  // max dynamic shared memory per vote block

@@ -81,3 +81,18 @@ def test_batch_request_without_votes(pkg, ctx, library):
     pose, _, _, _ = _alone(models[0], scenes[0][1])
     assert np.array_equal(poses[0], pose)
     assert stats[1]["n_kept"] == 0 and not poses[1].any()
+
+
+def test_registration_scenes_by_models_equals_lookups(pkg, ctx, library):
+    specs, _, _ = library
+    scenes = [specs[0].scene, specs[2].scene]
+    ms = [sp.models[0] for sp in specs]
+    ds = [sp.d_dists[0] for sp in specs]
+    poses, stats = pkg.ppf_registration(scenes, ms, ds, 5, 0.3, return_stats=True)
+    for i, sc in enumerate(scenes):
+        for j, (m, d) in enumerate(zip(ms, ds)):
+            model = pkg.Model(m, d, 0.3, context=ctx)
+            pose = model.ppf_lookup(pkg.Scene(sc, d, 5, context=ctx), raise_on_no_votes=False)
+            assert np.array_equal(poses[i][j], pose), (i, j)
+            assert stats[i][j]["n_votes"] == model.stats["n_votes"]
+            assert stats[i][j]["n_kept"] == model.stats["n_kept"]
