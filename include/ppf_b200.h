@@ -39,6 +39,7 @@ typedef enum ppf_status {
 typedef struct ppf_context_s* ppf_context_t; /* device + stream + workspace */
 typedef struct ppf_model_s* ppf_model_t;     /* resident model hash array */
 typedef struct ppf_scene_s* ppf_scene_t;     /* resident scene cloud */
+typedef struct ppf_server_s* ppf_server_t;   /* request loop over a model library */
 
 /* Per-lookup statistics (the reference logs these at debug level,
  * src/cuda/model.cu:122,152,161-168,280). */
@@ -116,6 +117,36 @@ ppf_status ppf_model_lookup(ppf_model_t m, ppf_scene_t s, float* pose_out, ppf_s
  * several requests; its inspection getters then show its last request. */
 ppf_status ppf_lookup_batch(ppf_context_t ctx, uint64_t n, const ppf_model_t* models,
                             const ppf_scene_t* scenes, float* poses_out, ppf_stats* stats_out);
+
+/* Request loop over a resident model library: a serving form of
+ * ppf_registration (src/cuda/ppf.cu:29-106), which instead rebuilds every
+ * model for every call.  The models stay owned by the caller and must
+ * outlive the server.  n_workers threads, each with its own context on
+ * `device`, take queued requests in arrival order and admit them while their
+ * estimated device memory (scene, candidate cells, lookup state) fits
+ * memory_budget bytes; up to max_batch admitted requests share one batched
+ * vote pass.  Workers run concurrently, so requests that arrive while others
+ * are on the GPU are admitted as memory frees and overlap them.  A request
+ * larger than the whole budget runs alone. */
+ppf_status ppf_server_create(int device, uint64_t n_models, const ppf_model_t* models,
+                             uint64_t memory_budget, uint32_t n_workers, uint32_t max_batch,
+                             ppf_server_t* out);
+/* Queues one scene (host memory, n x 3 points and normals, copied before the
+ * call returns) for registration against the library models model_ids[0..
+ * n_targets), each with its own d_dist as ppf_registration does.
+ * Thread-safe. */
+ppf_status ppf_server_submit(ppf_server_t srv, const float* xyz, const float* nxyz, uint64_t n,
+                             uint32_t ref_point_df, uint64_t n_targets, const uint32_t* model_ids,
+                             uint64_t* ticket);
+/* Waits for a request and collects it (a ticket is collected once):
+ * poses_out n_targets x 16 (host), stats_out n_targets records or NULL,
+ * latency_ms (may be NULL) from submission to completion.  Each pose equals
+ * ppf_model_lookup of the same (model, scene).  PPF_ERR_NO_VOTES when a
+ * target had no vote above the threshold (its pose is zero). */
+ppf_status ppf_server_wait(ppf_server_t srv, uint64_t ticket, float* poses_out, ppf_stats* stats_out,
+                           double* latency_ms);
+/* Finishes every queued request, then stops the workers. */
+ppf_status ppf_server_destroy(ppf_server_t srv);
 
 /* ppf_registration(scene_clouds, model_clouds, model_d_dists,
  * ref_point_downsample_factor, vote_count_threshold, cpu_clustering,

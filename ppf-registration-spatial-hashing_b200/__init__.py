@@ -15,6 +15,7 @@ from .api import (  # noqa: F401
     Model,
     PPFError,
     Scene,
+    Server,
     default_context,
     lookup_batch,
     pair_keys,

@@ -319,6 +319,61 @@ def pair_keys(cloud, d_dist: float, ref_point_downsample_factor: int = 1, contex
     return out.reshape(bp.n, bp.n)
 
 
+class Server:
+    """Request loop over a resident model library (ppf_server_*).
+
+    ``models`` are Model objects kept alive by the server.  ``submit`` queues a
+    scene (host arrays, copied before it returns) against library models by
+    index and returns a ticket; ``wait`` blocks for it and returns (poses
+    (k, 4, 4), stats, latency_ms).  Each pose equals Model.ppf_lookup of the
+    same (model, scene).  Submissions and waits may come from several threads.
+    """
+
+    def __init__(self, models, memory_budget: int = 40 << 30, workers: int = 2, max_batch: int = 16,
+                 device: int = 0):
+        self.models = list(models)
+        arr = (C.c_void_p * len(self.models))(*[m.handle for m in self.models])
+        h = C.c_void_p()
+        _check(_lib().ppf_server_create(int(device), len(self.models), arr, int(memory_budget), int(workers),
+                                        int(max_batch), C.byref(h)))
+        self.handle = h
+
+    def submit(self, cloud, model_ids, ref_point_downsample_factor: int = 1) -> int:
+        p, q = _split_cloud(cloud)
+        bp, bq = _Buf(p, "points"), _Buf(q, "normals")
+        if bp.n != bq.n:
+            raise ValueError("points and normals differ in length")
+        ids = np.ascontiguousarray(np.atleast_1d(model_ids), np.uint32)
+        t = C.c_uint64()
+        _check(_lib().ppf_server_submit(self.handle, bp.ptr, bq.ptr, bp.n, int(ref_point_downsample_factor),
+                                        ids.size, C.c_void_p(ids.ctypes.data), C.byref(t)))
+        self._targets = getattr(self, "_targets", {})
+        self._targets[t.value] = ids.size
+        return t.value
+
+    def wait(self, ticket: int, raise_on_no_votes: bool = True):
+        k = self._targets.pop(ticket, 1)
+        poses = np.zeros((k, 16), np.float32)
+        stats = (_capi.ppf_stats * k)()
+        lat = C.c_double()
+        status = _lib().ppf_server_wait(self.handle, int(ticket), C.c_void_p(poses.ctypes.data), stats,
+                                        C.byref(lat))
+        if not (status == 4 and not raise_on_no_votes):
+            _check(status)
+        return poses.reshape(k, 4, 4), [stats[i].as_dict() for i in range(k)], float(lat.value)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _lib().ppf_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def lookup_batch(models, scenes, context=None, return_stats: bool = False, raise_on_no_votes: bool = True):
     """Lookups of (models[i], scenes[i]) with one batched vote pass.
 

@@ -61,11 +61,7 @@ void copy_out(void* dst, const void* src_dev, size_t bytes, cudaStream_t st) {
   PPF_CUDA(cudaMemcpyAsync(dst, src_dev, bytes, cudaMemcpyDefault, st));
 }
 
-struct LookupOut {
-  ppf_status status = PPF_OK;
-  float pose[16] = {0};
-  ppf_stats stats{};
-};
+}  // namespace
 
 uint64_t model_signature(const Model& m) {
   uint32_t d, t;
@@ -77,13 +73,11 @@ uint64_t model_signature(const Model& m) {
 // The part of Model::ppf_lookup after the vote pass (threshold, order,
 // poses, clustering) and the pose extraction of ppf_registration, on the
 // candidate cells of one vote pass.  ev[2] marks the lookup's start.
-LookupOut finish_lookup(Model& m, const SceneData& s, const VoteResult& vr,
+LookupOut finish_lookup(Context& ctx, Model& m, LookupState& st, const SceneData& s, const VoteResult& vr,
                         const unsigned long long* cand_code, const uint32_t* cand_count,
-                        size_t launches0) {
-  Context& ctx = *m.ctx;
-  LookupState& st = m.last;
+                        size_t launches0, bool own_state) {
   LookupOut out;
-  m.cand_hint = vr.n_cand;
+  if (own_state) m.cand_hint = vr.n_cand;
   ctx.cand_hints[model_signature(m)] = vr.n_cand;
   st.U = 0;
   out.stats.n_votes = vr.n_votes;
@@ -143,15 +137,16 @@ LookupOut lookup(Model& m, const SceneData& s) {
   const size_t launches0 = ctx.launches;
   PPF_CUDA(cudaEventRecord(ctx.ev[2], ctx.stream));
   VoteResult vr = run_votes(ctx, m, s, false, -1.f);
-  return finish_lookup(m, s, vr, ctx.cand_codes.as<unsigned long long>(), ctx.cand_counts.as<uint32_t>(),
-                       launches0);
+  return finish_lookup(ctx, m, m.last, s, vr, ctx.cand_codes.as<unsigned long long>(),
+                       ctx.cand_counts.as<uint32_t>(), launches0, true);
 }
 
 // Several lookups with one batched vote pass: request i is (models[i],
 // scenes[i]).  Candidate buffers are sized from each model's last pass,
 // within a budget shared by the batch.
 std::vector<LookupOut> lookup_batch(Context& ctx, const std::vector<Model*>& models,
-                                    const std::vector<const SceneData*>& scenes) {
+                                    const std::vector<const SceneData*>& scenes, LookupState* states,
+                                    const size_t* caps) {
   const size_t n = models.size();
   const size_t launches0 = ctx.launches;
   PPF_CUDA(cudaEventRecord(ctx.ev[2], ctx.stream));
@@ -161,7 +156,7 @@ std::vector<LookupOut> lookup_batch(Context& ctx, const std::vector<Model*>& mod
   for (size_t i = 0; i < n; ++i) {
     reqs[i].m = models[i];
     reqs[i].s = scenes[i];
-    size_t hint = models[i]->cand_hint;
+    size_t hint = caps ? caps[i] : models[i]->cand_hint;
     if (!hint) {
       auto it = ctx.cand_hints.find(model_signature(*models[i]));
       if (it != ctx.cand_hints.end()) hint = it->second;
@@ -180,8 +175,10 @@ std::vector<LookupOut> lookup_batch(Context& ctx, const std::vector<Model*>& mod
   run_votes_batch(ctx, reqs);
   std::vector<LookupOut> out(n);
   for (size_t i = 0; i < n; ++i) {
-    out[i] = finish_lookup(*models[i], *scenes[i], reqs[i].r, reqs[i].codes.as<unsigned long long>(),
-                           reqs[i].counts.as<uint32_t>(), i == 0 ? launches0 : ctx.launches);
+    Model& m = *models[i];
+    out[i] = finish_lookup(ctx, m, states ? states[i] : m.last, *scenes[i], reqs[i].r,
+                           reqs[i].codes.as<unsigned long long>(), reqs[i].counts.as<uint32_t>(),
+                           i == 0 ? launches0 : ctx.launches, states == nullptr);
     PPF_CUDA(cudaEventRecord(ctx.ev[2], ctx.stream));
   }
   return out;
@@ -221,7 +218,6 @@ void init_context(Context& c, int device) {
   }
 }
 
-}  // namespace
 }  // namespace ppf
 
 using namespace ppf;
@@ -378,7 +374,7 @@ ppf_status ppf_lookup_batch(ppf_context_t ctx, uint64_t n, const ppf_model_t* mo
     }
     PPF_CUDA(cudaSetDevice(ctx->c.device));
     StreamScope scope(ctx->c.stream);
-    std::vector<LookupOut> r = lookup_batch(ctx->c, ms, ss);
+    std::vector<LookupOut> r = lookup_batch(ctx->c, ms, ss, nullptr, nullptr);
     std::vector<float> poses(n * 16);
     ppf_status worst = PPF_OK;
     for (uint64_t i = 0; i < n; ++i) {
@@ -388,6 +384,55 @@ ppf_status ppf_lookup_batch(ppf_context_t ctx, uint64_t n, const ppf_model_t* mo
     }
     PPF_CUDA(cudaMemcpy(poses_out, poses.data(), poses.size() * sizeof(float), cudaMemcpyDefault));
     if (worst != PPF_OK) return fail(worst, "no vote passed the threshold for at least one request");
+    return PPF_OK;
+  });
+}
+
+ppf_status ppf_server_create(int device, uint64_t n_models, const ppf_model_t* models,
+                             uint64_t memory_budget, uint32_t n_workers, uint32_t max_batch,
+                             ppf_server_t* out) {
+  return guarded([&]() {
+    PPF_REQUIRE(out && models && n_models, PPF_ERR_INVALID_ARGUMENT, "null output or empty library");
+    std::vector<Model*> ms(n_models);
+    for (uint64_t j = 0; j < n_models; ++j) {
+      PPF_REQUIRE(models[j], PPF_ERR_INVALID_ARGUMENT, "null model in the library");
+      ms[j] = &models[j]->m;
+    }
+    std::unique_ptr<ppf_server_s> s(new ppf_server_s());
+    s->srv = server_create(device, ms, memory_budget, n_workers, max_batch);
+    *out = s.release();
+    return PPF_OK;
+  });
+}
+
+ppf_status ppf_server_submit(ppf_server_t srv, const float* xyz, const float* nxyz, uint64_t n,
+                             uint32_t ref_point_df, uint64_t n_targets, const uint32_t* model_ids,
+                             uint64_t* ticket) {
+  return guarded([&]() {
+    PPF_REQUIRE(srv && srv->srv && ticket, PPF_ERR_INVALID_ARGUMENT, "null server or ticket");
+    *ticket = server_submit(srv->srv, xyz, nxyz, n, ref_point_df, model_ids, n_targets);
+    return PPF_OK;
+  });
+}
+
+ppf_status ppf_server_wait(ppf_server_t srv, uint64_t ticket, float* poses_out, ppf_stats* stats_out,
+                           double* latency_ms) {
+  return guarded([&]() {
+    PPF_REQUIRE(srv && srv->srv, PPF_ERR_INVALID_ARGUMENT, "null server");
+    std::string err;
+    const ppf_status st = server_wait(srv->srv, ticket, poses_out, stats_out, latency_ms, &err);
+    if (st != PPF_OK)
+      return fail(st, err.empty() ? "no vote passed the threshold for at least one target" : err);
+    return PPF_OK;
+  });
+}
+
+ppf_status ppf_server_destroy(ppf_server_t srv) {
+  return guarded([&]() {
+    if (srv) {
+      if (srv->srv) server_destroy(srv->srv);
+      delete srv;
+    }
     return PPF_OK;
   });
 }
@@ -454,7 +499,7 @@ ppf_status ppf_registration(ppf_context_t ctx, uint64_t n_scenes, const float* c
           ss.push_back(&s->s);
           slot.push_back(i * n_models + j);
         }
-      std::vector<LookupOut> r = lookup_batch(c->c, ms, ss);
+      std::vector<LookupOut> r = lookup_batch(c->c, ms, ss, nullptr, nullptr);
       for (size_t k = 0; k < r.size(); ++k) {
         std::memcpy(&host_poses[slot[k] * 16], r[k].pose, sizeof(r[k].pose));
         if (stats_out) stats_out[slot[k]] = r[k].stats;

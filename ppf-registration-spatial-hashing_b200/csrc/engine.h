@@ -2,6 +2,7 @@
 // resident scenes, and the device-side layout the kernels consume.
 #pragma once
 
+#include <string>
 #include <unordered_map>
 #include <vector>
 
@@ -172,6 +173,30 @@ void compute_poses(Context& ctx, const Model& m, const SceneData& s, LookupState
 // GPU clustering + argmax; writes the best pose into st.best and returns the index.
 size_t cluster_poses_gpu(Context& ctx, const Model& m, LookupState& st, float* best_score);
 
+// ---- lookups (capi.cu)
+struct LookupOut {
+  ppf_status status = PPF_OK;
+  float pose[16] = {0};
+  ppf_stats stats{};
+};
+void init_context(Context& c, int device);
+// Lookups of (models[i], scenes[i]) with one batched vote pass.  states:
+// per-request lookup state (nullptr: each model's own `last`); caps:
+// per-request candidate capacity hints (nullptr: the models' last passes).
+std::vector<LookupOut> lookup_batch(Context& ctx, const std::vector<Model*>& models,
+                                    const std::vector<const SceneData*>& scenes, LookupState* states,
+                                    const size_t* caps);
+
+// ---- request loop (serve.cu)
+struct Server;
+Server* server_create(int device, const std::vector<Model*>& models, size_t memory_budget,
+                      uint32_t n_workers, uint32_t max_batch);
+uint64_t server_submit(Server* srv, const float* xyz, const float* nxyz, uint64_t n, uint32_t ref_df,
+                       const uint32_t* model_ids, uint64_t n_ids);
+ppf_status server_wait(Server* srv, uint64_t ticket, float* poses, ppf_stats* stats, double* latency_ms,
+                       std::string* error);
+void server_destroy(Server* srv);
+
 // ---- greedy CPU clustering (cpu_cluster.cpp)
 int cluster_poses_cpu(const float* poses, const uint32_t* votes, size_t n, float trans_thresh,
                       float rot_thresh, float out_poses[3 * 16], uint32_t out_votes[3]);
@@ -187,4 +212,7 @@ struct ppf_model_s {
 struct ppf_scene_s {
   ppf::Context* ctx = nullptr;
   ppf::SceneData s;
+};
+struct ppf_server_s {
+  ppf::Server* srv = nullptr;
 };
