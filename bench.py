@@ -199,6 +199,107 @@ def run_reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def run_serve(args):
+    """Library workload: 8 models (2k-6k points by default, tau_d = 0.04),
+    scenes (5k-40k points by default) each holding 1-4 of them; a request
+    registers one scene against the models it holds (ref_point_df=5,
+    threshold 0.3).
+
+    plain  : one ppf_registration per request, rebuilding its models (the
+             reference's per-call behaviour), requests one after another.
+    batched: resident library; all requests in one ppf_lookup_batch.
+    served : resident library behind the request loop (2 workers); requests
+             arrive as a seeded Poisson process, at 70% of the batched rate
+             (latency under load) and at 150% (capacity: the queue stays full).
+    Every served pose is compared with the plain pose of the same pair."""
+    import threading
+
+    pkg = ge.load_package()
+    models, d_dists, scenes = pkg.synthetic.config_library(
+        seed=1003, n_models=8, n_scenes=args.serve_scenes, model_range=tuple(args.serve_model_range),
+        scene_range=tuple(args.serve_scene_range))
+    ctx = pkg.Context(0)
+    reqs = [(sc, sorted({i.model_index for i in inst})) for sc, inst in scenes]
+    n_reg = sum(len(ids) for _, ids in reqs)
+
+    def plain_all():
+        out = []
+        for sc, ids in reqs:
+            p = pkg.ppf_registration([sc], [models[j] for j in ids], [d_dists[j] for j in ids], REF_DF, THR,
+                                     context=ctx)
+            out.append(np.asarray(p[0]))
+        return out
+
+    plain_all()  # warm-up (pool, hints)
+    ctx.synchronize()
+    t0 = time.perf_counter()
+    plain = plain_all()
+    ctx.synchronize()
+    t_plain = time.perf_counter() - t0
+
+    lib = [pkg.Model(m, d, THR, context=ctx) for m, d in zip(models, d_dists)]
+
+    def batched_all():
+        ms, ss = [], []
+        for sc, ids in reqs:
+            for j in ids:
+                ms.append(lib[j])
+                ss.append(pkg.Scene(sc, d_dists[j], REF_DF, context=ctx))
+        return pkg.lookup_batch(ms, ss, context=ctx, raise_on_no_votes=False)
+
+    batched_all()
+    ctx.synchronize()
+    t0 = time.perf_counter()
+    batched_all()
+    ctx.synchronize()
+    t_batch = time.perf_counter() - t0
+
+    srv = pkg.Server(lib, workers=2, max_batch=16)
+    for t in [srv.submit(sc, ids, REF_DF) for sc, ids in reqs[:4]]:
+        srv.wait(t, raise_on_no_votes=False)
+
+    def serve_at(load, seed):
+        rate = load * len(reqs) / t_batch  # requests/s offered
+        arrivals = np.cumsum(np.random.default_rng(seed).exponential(1.0 / rate, len(reqs)))
+        tickets = [None] * len(reqs)
+
+        def submitter():
+            start = time.perf_counter()
+            for i, (sc, ids) in enumerate(reqs):
+                d = start + arrivals[i] - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                tickets[i] = srv.submit(sc, ids, REF_DF)
+
+        t0 = time.perf_counter()
+        th = threading.Thread(target=submitter)
+        th.start()
+        th.join()
+        res = [srv.wait(t, raise_on_no_votes=False) for t in tickets]
+        t_serve = time.perf_counter() - t0
+        lat = np.array([r[2] for r in res])
+        same = sum(int(np.array_equal(r[0], plain[i])) for i, r in enumerate(res))
+        return {"offered_requests_per_s": rate, "registrations_per_s": n_reg / t_serve,
+                "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                "identical_poses_vs_plain": f"{same}/{len(reqs)}"}
+
+    light = serve_at(0.7, 7)
+    heavy = serve_at(1.5, 8)
+    srv.close()
+    line = {"mode": "serve", "metric": METRIC, "unit": METRIC, "higher_is_better": True, "n_gpus": 1,
+            "plain": n_reg / t_plain, "batched": n_reg / t_batch, "served": heavy["registrations_per_s"],
+            "batched_over_plain": t_plain / t_batch,
+            "served_over_plain": heavy["registrations_per_s"] / (n_reg / t_plain),
+            "served_at_70pct": light, "served_at_150pct": heavy,
+            "requests": len(reqs), "registrations": n_reg, "data": "synthetic", "dtype": "f32",
+            "config": {"workload": f"library of 8 models ({args.serve_model_range[0]}-{args.serve_model_range[1]} "
+                                   f"pts, tau_d=0.04), {len(reqs)} scenes of {args.serve_scene_range[0]}-"
+                                   f"{args.serve_scene_range[1]} pts holding 1-4 models each, ref_point_df=5, "
+                                   "threshold 0.3",
+                       "served": "2 workers, max_batch 16, Poisson arrivals at 70% and 150% of the batched rate"}}
+    print(json.dumps(line), flush=True)
+
+
 def run_profile_case(args):
     """One lookup of model 0 against the scene at ref_point_df=50."""
     pkg, spec = workload()
@@ -228,6 +329,12 @@ def main():
     ap.add_argument("--clock-interval-ms", type=int, default=2500,
                     help="nvidia-smi sampling interval during the timed region (each query stalls the "
                          "engine's CUDA calls briefly)")
+    ap.add_argument("--serve", action="store_true",
+                    help="library workload: plain per-request registration vs batched lookups vs the "
+                         "request loop under Poisson arrivals (p50/p99 latency)")
+    ap.add_argument("--serve-scenes", type=int, default=64)
+    ap.add_argument("--serve-model-range", type=int, nargs=2, default=(2000, 6000))
+    ap.add_argument("--serve-scene-range", type=int, nargs=2, default=(5000, 40000))
     ap.add_argument("--profile-case", action="store_true",
                     help="one lookup of model 0 at ref_point_df=50 (short vote launch for ncu)")
     args = ap.parse_args()
@@ -235,6 +342,8 @@ def main():
         return run_reference_arm(args)
     if args.profile_case:
         return run_profile_case(args)
+    if args.serve:
+        return run_serve(args)
 
     import torch
 
