@@ -118,6 +118,24 @@ ppf_status ppf_model_lookup(ppf_model_t m, ppf_scene_t s, float* pose_out, ppf_s
 ppf_status ppf_lookup_batch(ppf_context_t ctx, uint64_t n, const ppf_model_t* models,
                             const ppf_scene_t* scenes, float* poses_out, ppf_stats* stats_out);
 
+/* pcl::getMinMax3D of a cloud as the alignment driver uses it
+ * (src/alignment.cpp:246-253): per-axis minimum and maximum over the finite
+ * points of n x 3 xyz (host or device).  The driver's model d_dist is
+ * tau_d * max(max - min).  PPF_ERR_INVALID_ARGUMENT when no point is finite. */
+ppf_status ppf_cloud_extent(ppf_context_t ctx, const float* xyz, uint64_t n, float* min_out,
+                            float* max_out);
+
+/* voxelGridDownsample (src/alignment.cpp:79-87): pcl::VoxelGrid<PointNormal>
+ * (PCL 1.8) with cubic leaf size `leaf`.  Non-empty voxels in the grid's
+ * linear index order (x fastest), each the mean of its points' coordinates
+ * and normals (normals are not renormalised); the input is returned
+ * unchanged when the grid would exceed 2^31 - 1 cells, as PCL does.  Inputs
+ * and outputs host or device; outputs need room for *n_out <= n points
+ * (cap); PPF_ERR_INVALID_ARGUMENT with *n_out set when cap is smaller. */
+ppf_status ppf_voxel_downsample(ppf_context_t ctx, const float* xyz, const float* nxyz, uint64_t n,
+                                float leaf, float* out_xyz, float* out_nxyz, uint64_t cap,
+                                uint64_t* n_out);
+
 /* Request loop over a resident model library: a serving form of
  * ppf_registration (src/cuda/ppf.cu:29-106), which instead rebuilds every
  * model for every call.  The models stay owned by the caller and must

@@ -108,6 +108,9 @@ class Oracle:
         L.orc_vote_counts.argtypes = [_u32p, C.c_int64, _u32p, _u32p, C.c_int64, _u64p]
         L.orc_cluster_poses.restype = C.c_int
         L.orc_cluster_poses.argtypes = [_fp, _u32p, C.c_int64, C.c_float, C.c_float, _fp, _u32p]
+        L.orc_cloud_extent.argtypes = [_fp, C.c_int64, _fp, _fp]
+        L.orc_voxel_downsample.argtypes = [_fp, _fp, C.c_int64, C.c_float, _fp, _fp]
+        L.orc_voxel_downsample.restype = C.c_int64
         self.L = L
 
     # -- single items
@@ -219,6 +222,19 @@ class Oracle:
         nc = self.L.orc_cluster_poses(_p(P), _p(v, _u32p), v.size, float(trans_thresh), float(rot_thresh),
                                       _p(out), _p(ov, _u32p))
         return out.reshape(3, 4, 4)[:nc], ov[:nc]
+
+
+    def cloud_extent(self, xyz):
+        p = _f32(xyz)
+        lo, hi = np.zeros(3, np.float32), np.zeros(3, np.float32)
+        ok = self.L.orc_cloud_extent(_p(p), p.shape[0], _p(lo), _p(hi))
+        return (lo, hi) if ok else None
+
+    def voxel_downsample(self, xyz, nxyz, leaf):
+        p, q = _f32(xyz), _f32(nxyz)
+        ox, on = np.zeros_like(p), np.zeros_like(q)
+        k = self.L.orc_voxel_downsample(_p(p), _p(q), p.shape[0], float(leaf), _p(ox), _p(on))
+        return ox[:k], on[:k]
 
 
 class RefHost:

@@ -823,3 +823,76 @@ void orc_result_free(orc_result* r) {
 }
 
 }  // extern "C"
+
+/* ---- driver preprocessing ---- */
+
+int orc_cloud_extent(const float* xyz, int64_t n, float lo[3], float hi[3]) {
+  int any = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    const float* p = xyz + 3 * i;
+    if (!std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2])) continue;
+    for (int k = 0; k < 3; ++k) {
+      if (!any || p[k] < lo[k]) lo[k] = p[k];
+      if (!any || p[k] > hi[k]) hi[k] = p[k];
+    }
+    any = 1;
+  }
+  return any;
+}
+
+/* pcl::VoxelGrid<PointT>::applyFilter (PCL 1.8) as the alignment driver
+ * calls it (src/alignment.cpp:79-87): min/max bounding box in leaf units,
+ * linear index per finite point, sort by index, mean of each voxel. */
+int64_t orc_voxel_downsample(const float* xyz, const float* nxyz, int64_t n, float leaf, float* out_xyz,
+                             float* out_nxyz) {
+  float lo[3], hi[3];
+  if (!orc_cloud_extent(xyz, n, lo, hi)) return 0;
+  const float inv = 1.0f / leaf;
+  long long d[3];
+  for (int k = 0; k < 3; ++k) d[k] = (long long)((hi[k] - lo[k]) * inv) + 1;
+  if (d[0] * d[1] * d[2] > (long long)INT32_MAX) {
+    std::memcpy(out_xyz, xyz, (size_t)n * 12);
+    std::memcpy(out_nxyz, nxyz, (size_t)n * 12);
+    return n;
+  }
+  int min_b[3], max_b[3];
+  for (int k = 0; k < 3; ++k) {
+    min_b[k] = (int)std::floor(lo[k] * inv);
+    max_b[k] = (int)std::floor(hi[k] * inv);
+  }
+  const long long dx = max_b[0] - min_b[0] + 1, dy = max_b[1] - min_b[1] + 1;
+  std::vector<std::pair<uint32_t, int64_t>> iv;
+  iv.reserve((size_t)n);
+  for (int64_t i = 0; i < n; ++i) {
+    const float* p = xyz + 3 * i;
+    if (!std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2])) continue;
+    int ijk[3];
+    for (int k = 0; k < 3; ++k) ijk[k] = (int)(std::floor(p[k] * inv) - (float)min_b[k]);
+    iv.push_back({(uint32_t)(ijk[0] + ijk[1] * (int)dx + ijk[2] * (int)(dx * dy)), i});
+  }
+  std::stable_sort(iv.begin(), iv.end(),
+                   [](const std::pair<uint32_t, int64_t>& a, const std::pair<uint32_t, int64_t>& b) {
+                     return a.first < b.first;
+                   });
+  int64_t K = 0;
+  for (size_t a = 0; a < iv.size();) {
+    size_t b = a;
+    float s[6] = {0, 0, 0, 0, 0, 0};
+    while (b < iv.size() && iv[b].first == iv[a].first) {
+      const int64_t p = iv[b].second;
+      for (int k = 0; k < 3; ++k) {
+        s[k] += xyz[3 * p + k];
+        s[3 + k] += nxyz[3 * p + k];
+      }
+      ++b;
+    }
+    const float c = (float)(b - a);
+    for (int k = 0; k < 3; ++k) {
+      out_xyz[3 * K + k] = s[k] / c;
+      out_nxyz[3 * K + k] = s[3 + k] / c;
+    }
+    ++K;
+    a = b;
+  }
+  return K;
+}

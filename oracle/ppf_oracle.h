@@ -122,6 +122,19 @@ void orc_vote_counts(const uint32_t* scene_keys, int64_t n, const uint32_t* uniq
 int orc_cluster_poses(const float* poses, const uint32_t* votes, int64_t n, float trans_thresh,
                       float rot_thresh, float out_poses[3 * 16], uint32_t out_votes[3]);
 
+/* ---- driver preprocessing (src/alignment.cpp:79-87, 246-253) ---- */
+
+/* pcl::getMinMax3D over the finite points; returns 0 when there is none. */
+int orc_cloud_extent(const float* xyz, int64_t n, float lo[3], float hi[3]);
+
+/* pcl::VoxelGrid<PointNormal> (PCL 1.8, restated from its published
+ * algorithm) with leaf size `leaf`: voxel means of points and normals in
+ * linear voxel order, each voxel summed in input order; out arrays need room
+ * for n points.  Returns the number of voxels (n, with the input copied, when
+ * the grid exceeds 2^31 - 1 cells). */
+int64_t orc_voxel_downsample(const float* xyz, const float* nxyz, int64_t n, float leaf, float* out_xyz,
+                             float* out_nxyz);
+
 #ifdef __cplusplus
 }
 #endif

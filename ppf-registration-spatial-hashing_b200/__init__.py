@@ -16,6 +16,10 @@ from .api import (  # noqa: F401
     PPFError,
     Scene,
     Server,
+    cloud_extent,
+    model_d_dist,
+    preprocess,
+    voxel_downsample,
     default_context,
     lookup_batch,
     pair_keys,

@@ -319,6 +319,52 @@ def pair_keys(cloud, d_dist: float, ref_point_downsample_factor: int = 1, contex
     return out.reshape(bp.n, bp.n)
 
 
+def cloud_extent(cloud, context=None):
+    """pcl::getMinMax3D of a cloud's points (finite ones): (min[3], max[3])."""
+    ctx = context or default_context()
+    p, _ = _split_cloud(cloud) if isinstance(cloud, (tuple, list)) or hasattr(cloud, "points") else (cloud, None)
+    bp = _Buf(p, "points")
+    lo, hi = np.zeros(3, np.float32), np.zeros(3, np.float32)
+    _check(_lib().ppf_cloud_extent(ctx.handle, bp.ptr, bp.n, C.c_void_p(lo.ctypes.data), C.c_void_p(hi.ctypes.data)))
+    return lo, hi
+
+
+def model_d_dist(cloud, tau_d: float, context=None) -> float:
+    """The alignment driver's d_dist of a model: tau_d times its largest
+    axis-aligned extent, in float32 (src/alignment.cpp:246-253)."""
+    lo, hi = cloud_extent(cloud, context)
+    return float(np.float32(tau_d) * np.max(hi - lo))
+
+
+def voxel_downsample(cloud, leaf: float, context=None):
+    """voxelGridDownsample (src/alignment.cpp:79-87, pcl::VoxelGrid with a
+    cubic leaf): (points, normals) of the voxel means, as float32 numpy."""
+    ctx = context or default_context()
+    p, q = _split_cloud(cloud)
+    bp, bq = _Buf(p, "points"), _Buf(q, "normals")
+    if bp.n != bq.n:
+        raise ValueError("points and normals differ in length")
+    ox = np.zeros((max(bp.n, 1), 3), np.float32)
+    on = np.zeros((max(bp.n, 1), 3), np.float32)
+    k = C.c_uint64()
+    _check(_lib().ppf_voxel_downsample(ctx.handle, bp.ptr, bq.ptr, bp.n, float(leaf), C.c_void_p(ox.ctypes.data),
+                                       C.c_void_p(on.ctypes.data), bp.n, C.byref(k)))
+    return ox[: k.value].copy(), on[: k.value].copy()
+
+
+def preprocess(scene_clouds, model_clouds, tau_d, scene_leaf_size: float, context=None):
+    """The alignment driver's preparation (src/alignment.cpp:203-288): each
+    model's d_dist from its extent and tau_d, scenes downsampled with
+    scene_leaf_size, each model with its own d_dist.  Returns (scenes,
+    models, model_d_dists) with clouds as (points, normals) pairs."""
+    if len(tau_d) != len(model_clouds):
+        raise ValueError("each model must have an associated tau_d")
+    d_dists = [model_d_dist(m, t, context) for m, t in zip(model_clouds, tau_d)]
+    scenes = [voxel_downsample(s, scene_leaf_size, context) for s in scene_clouds]
+    models = [voxel_downsample(m, d, context) for m, d in zip(model_clouds, d_dists)]
+    return scenes, models, d_dists
+
+
 class Server:
     """Request loop over a resident model library (ppf_server_*).
 

@@ -388,6 +388,52 @@ ppf_status ppf_lookup_batch(ppf_context_t ctx, uint64_t n, const ppf_model_t* mo
   });
 }
 
+namespace {
+// n x 3 floats on the device: the caller's pointer, or a copy of host memory
+const float* device_xyz(Context& c, const float* p, size_t n, DevBuf& tmp) {
+  if (is_device_pointer(p)) return p;
+  tmp.reserve(std::max<size_t>(n, 1) * 12);
+  if (n) PPF_CUDA(cudaMemcpyAsync(tmp.ptr, p, n * 12, cudaMemcpyHostToDevice, c.stream));
+  return tmp.as<float>();
+}
+}  // namespace
+
+ppf_status ppf_cloud_extent(ppf_context_t ctx, const float* xyz, uint64_t n, float* min_out, float* max_out) {
+  return guarded([&]() {
+    PPF_REQUIRE(ctx && xyz && min_out && max_out, PPF_ERR_INVALID_ARGUMENT, "null argument");
+    PPF_CUDA(cudaSetDevice(ctx->c.device));
+    StreamScope scope(ctx->c.stream);
+    DevBuf tmp;
+    const float* d = device_xyz(ctx->c, xyz, n, tmp);
+    float lo[3], hi[3];
+    PPF_REQUIRE(cloud_extent(ctx->c, d, n, lo, hi), PPF_ERR_INVALID_ARGUMENT, "no finite point");
+    std::memcpy(min_out, lo, sizeof(lo));
+    std::memcpy(max_out, hi, sizeof(hi));
+    return PPF_OK;
+  });
+}
+
+ppf_status ppf_voxel_downsample(ppf_context_t ctx, const float* xyz, const float* nxyz, uint64_t n, float leaf,
+                                float* out_xyz, float* out_nxyz, uint64_t cap, uint64_t* n_out) {
+  return guarded([&]() {
+    PPF_REQUIRE(ctx && xyz && nxyz && n_out, PPF_ERR_INVALID_ARGUMENT, "null argument");
+    PPF_CUDA(cudaSetDevice(ctx->c.device));
+    StreamScope scope(ctx->c.stream);
+    DevBuf ta, tb, ox, on;
+    const float* dx = device_xyz(ctx->c, xyz, n, ta);
+    const float* dn = device_xyz(ctx->c, nxyz, n, tb);
+    const size_t K = voxel_downsample(ctx->c, dx, dn, n, leaf, ox, on);
+    *n_out = K;
+    PPF_REQUIRE(K <= cap, PPF_ERR_INVALID_ARGUMENT,
+                "output capacity " + std::to_string(cap) + " below the " + std::to_string(K) + " voxels");
+    PPF_REQUIRE(!K || (out_xyz && out_nxyz), PPF_ERR_INVALID_ARGUMENT, "null output");
+    copy_out(out_xyz, ox.ptr, K * 12, ctx->c.stream);
+    copy_out(out_nxyz, on.ptr, K * 12, ctx->c.stream);
+    PPF_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    return PPF_OK;
+  });
+}
+
 ppf_status ppf_server_create(int device, uint64_t n_models, const ppf_model_t* models,
                              uint64_t memory_budget, uint32_t n_workers, uint32_t max_batch,
                              ppf_server_t* out) {

@@ -173,6 +173,13 @@ void compute_poses(Context& ctx, const Model& m, const SceneData& s, LookupState
 // GPU clustering + argmax; writes the best pose into st.best and returns the index.
 size_t cluster_poses_gpu(Context& ctx, const Model& m, LookupState& st, float* best_score);
 
+// ---- driver preprocessing (preprocess.cu)
+// per-axis min / max over finite points (false when there is none)
+bool cloud_extent(Context& ctx, const float* xyz_dev, size_t n, float lo[3], float hi[3]);
+// pcl::VoxelGrid centroids of an n x 3 cloud; returns the voxel count
+size_t voxel_downsample(Context& ctx, const float* xyz_dev, const float* nxyz_dev, size_t n, float leaf,
+                        DevBuf& out_xyz, DevBuf& out_nxyz);
+
 // ---- lookups (capi.cu)
 struct LookupOut {
   ppf_status status = PPF_OK;
