@@ -118,6 +118,15 @@ ppf_status ppf_model_lookup(ppf_model_t m, ppf_scene_t s, float* pose_out, ppf_s
 ppf_status ppf_lookup_batch(ppf_context_t ctx, uint64_t n, const ppf_model_t* models,
                             const ppf_scene_t* scenes, float* poses_out, ppf_stats* stats_out);
 
+/* pcl::io::loadPLYFile<pcl::PointNormal> as the alignment driver loads its
+ * scene and model files (src/alignment.cpp:212,241): the vertex element's x,
+ * y, z and nx, ny, nz (or normal_x, normal_y, normal_z), any scalar type,
+ * ascii or binary files; other elements are skipped.  xyz, nxyz: host arrays
+ * of cap x 3 floats.  With cap = 0 and null arrays only *n_out is set. */
+ppf_status ppf_ply_read(const char* path, float* xyz, float* nxyz, uint64_t cap, uint64_t* n_out);
+/* Writes a binary_little_endian PLY of float x y z nx ny nz (host arrays). */
+ppf_status ppf_ply_write(const char* path, const float* xyz, const float* nxyz, uint64_t n);
+
 /* pcl::getMinMax3D of a cloud as the alignment driver uses it
  * (src/alignment.cpp:246-253): per-axis minimum and maximum over the finite
  * points of n x 3 xyz (host or device).  The driver's model d_dist is

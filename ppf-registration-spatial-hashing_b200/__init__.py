@@ -17,6 +17,11 @@ from .api import (  # noqa: F401
     Scene,
     Server,
     cloud_extent,
+    ht_dist,
+    load_ply,
+    load_xf,
+    save_ply,
+    validate,
     model_d_dist,
     preprocess,
     voxel_downsample,

@@ -88,6 +88,8 @@ SIGNATURES = {
     "ppf_model_all_votes": (C.c_int, [_vp, _vp, _u64p, _u32p, C.c_uint64, _u64p]),
     "ppf_model_pair_vote_counts": (C.c_int, [_vp, _vp, _vp]),
     "ppf_lookup_batch": (C.c_int, [_vp, C.c_uint64, _vp, _vp, _vp, _vp]),
+    "ppf_ply_read": (C.c_int, [C.c_char_p, _vp, _vp, C.c_uint64, _u64p]),
+    "ppf_ply_write": (C.c_int, [C.c_char_p, _vp, _vp, C.c_uint64]),
     "ppf_cloud_extent": (C.c_int, [_vp, _vp, C.c_uint64, _vp, _vp]),
     "ppf_voxel_downsample": (C.c_int, [_vp, _vp, _vp, C.c_uint64, C.c_float, _vp, _vp, C.c_uint64, _u64p]),
     "ppf_server_create": (C.c_int, [C.c_int, C.c_uint64, _vp, C.c_uint64, C.c_uint32, C.c_uint32, _vp]),

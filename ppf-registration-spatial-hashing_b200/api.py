@@ -319,6 +319,83 @@ def pair_keys(cloud, d_dist: float, ref_point_downsample_factor: int = 1, contex
     return out.reshape(bp.n, bp.n)
 
 
+def load_ply(path):
+    """pcl::io::loadPLYFile<PointNormal> as the alignment driver uses it
+    (src/alignment.cpp:212,241): (points, normals) float32 (n, 3)."""
+    L = _lib()
+    p = str(path).encode()
+    n = C.c_uint64()
+    _check(L.ppf_ply_read(p, None, None, 0, C.byref(n)))
+    xyz = np.zeros((max(n.value, 1), 3), np.float32)
+    nrm = np.zeros((max(n.value, 1), 3), np.float32)
+    _check(L.ppf_ply_read(p, C.c_void_p(xyz.ctypes.data), C.c_void_p(nrm.ctypes.data), n.value, C.byref(n)))
+    return xyz[: n.value], nrm[: n.value]
+
+
+def save_ply(path, cloud):
+    """Writes a binary little-endian PLY of float x y z nx ny nz."""
+    p, q = _split_cloud(cloud)
+    p = np.ascontiguousarray(np.asarray(p, np.float32))
+    q = np.ascontiguousarray(np.asarray(q, np.float32))
+    _check(_lib().ppf_ply_write(str(path).encode(), C.c_void_p(p.ctypes.data), C.c_void_p(q.ctypes.data), len(p)))
+
+
+def load_xf(path) -> np.ndarray:
+    """A ground-truth pose file (.xf) as the driver reads it into an
+    Eigen::Matrix4f (src/alignment.cpp:306-307): 16 numbers, row-major."""
+    vals = np.array(open(path).read().split(), dtype=np.float64)
+    if vals.size < 16:
+        raise ValueError(f"{path}: expected 16 numbers")
+    return vals[:16].reshape(4, 4).astype(np.float32)
+
+
+def _quat(R):
+    """Unit quaternion (w, x, y, z) of a rotation matrix (largest-component branch)."""
+    R = np.asarray(R, np.float64)
+    t = np.trace(R)
+    if t > 0:
+        s = np.sqrt(t + 1.0) * 2
+        q = [0.25 * s, (R[2, 1] - R[1, 2]) / s, (R[0, 2] - R[2, 0]) / s, (R[1, 0] - R[0, 1]) / s]
+    else:
+        i = int(np.argmax(np.diag(R)))
+        j, k = (i + 1) % 3, (i + 2) % 3
+        s = np.sqrt(1.0 + R[i, i] - R[j, j] - R[k, k]) * 2
+        q = [0.0, 0.0, 0.0, 0.0]
+        q[0] = (R[k, j] - R[j, k]) / s
+        q[1 + i] = 0.25 * s
+        q[1 + j] = (R[j, i] + R[i, j]) / s
+        q[1 + k] = (R[k, i] + R[i, k]) / s
+    q = np.array(q)
+    return q / np.linalg.norm(q)
+
+
+def ht_dist(a, b):
+    """ht_dist (src/cuda/linalg.cu:9-20): (|t_a - t_b|, rotation angle of
+    R_a^-1 R_b in [0, pi]) of two 4x4 poses.  The reference takes the angle
+    from Eigen's AngleAxis of the quaternion product, 2 atan2(|v|, |w|);
+    Eigen is not installed here, so the same quantity is restated in float64
+    (the translation distance is taken in float32, as the reference does)."""
+    a = np.asarray(a, np.float32).reshape(4, 4)
+    b = np.asarray(b, np.float32).reshape(4, 4)
+    d = a[:3, 3] - b[:3, 3]
+    td = float(np.sqrt(np.float32(d[0] * d[0] + d[1] * d[1] + d[2] * d[2])))
+    qa, qb = _quat(a[:3, :3]), _quat(b[:3, :3])
+    w = qa[0] * qb[0] + np.dot(qa[1:], qb[1:])  # (qa^-1 qb).w
+    v = qa[0] * qb[1:] - qb[0] * qa[1:] - np.cross(qa[1:], qb[1:])
+    return td, float(abs(2.0 * np.arctan2(np.linalg.norm(v), abs(w))))
+
+
+def validate(pose, truth, model_diameter: float, translation_threshold: float = 0.1,
+             rotation_threshold_deg: float = 12.0):
+    """The driver's validation (src/alignment.cpp:300-335): a pose matches when
+    its translation is within translation_threshold * model_diameter of the
+    ground truth and its rotation within rotation_threshold_deg.  Returns
+    (match, (translation distance, rotation angle))."""
+    td, rd = ht_dist(pose, truth)
+    ok = td < translation_threshold * model_diameter and rd < np.deg2rad(rotation_threshold_deg)
+    return bool(ok), (td, rd)
+
+
 def cloud_extent(cloud, context=None):
     """pcl::getMinMax3D of a cloud's points (finite ones): (min[3], max[3])."""
     ctx = context or default_context()

@@ -434,6 +434,23 @@ ppf_status ppf_voxel_downsample(ppf_context_t ctx, const float* xyz, const float
   });
 }
 
+ppf_status ppf_ply_read(const char* path, float* xyz, float* nxyz, uint64_t cap, uint64_t* n_out) {
+  return guarded([&]() {
+    std::string err;
+    const ppf_status st = ply_read(path, xyz, nxyz, cap, n_out, &err);
+    if (st != PPF_OK) return fail(st, err);
+    return PPF_OK;
+  });
+}
+
+ppf_status ppf_ply_write(const char* path, const float* xyz, const float* nxyz, uint64_t n) {
+  return guarded([&]() {
+    const ppf_status st = ply_write(path, xyz, nxyz, n);
+    if (st != PPF_OK) return fail(st, std::string("cannot write ") + (path ? path : "(null)"));
+    return PPF_OK;
+  });
+}
+
 ppf_status ppf_server_create(int device, uint64_t n_models, const ppf_model_t* models,
                              uint64_t memory_budget, uint32_t n_workers, uint32_t max_batch,
                              ppf_server_t* out) {

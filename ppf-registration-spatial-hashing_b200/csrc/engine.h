@@ -180,6 +180,10 @@ bool cloud_extent(Context& ctx, const float* xyz_dev, size_t n, float lo[3], flo
 size_t voxel_downsample(Context& ctx, const float* xyz_dev, const float* nxyz_dev, size_t n, float leaf,
                         DevBuf& out_xyz, DevBuf& out_nxyz);
 
+// ---- PLY files (ply.cpp)
+ppf_status ply_read(const char* path, float* xyz, float* nxyz, uint64_t cap, uint64_t* n_out, std::string* err);
+ppf_status ply_write(const char* path, const float* xyz, const float* nxyz, uint64_t n);
+
 // ---- lookups (capi.cu)
 struct LookupOut {
   ppf_status status = PPF_OK;
