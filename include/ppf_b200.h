@@ -118,6 +118,18 @@ ppf_status ppf_model_lookup(ppf_model_t m, ppf_scene_t s, float* pose_out, ppf_s
 ppf_status ppf_lookup_batch(ppf_context_t ctx, uint64_t n, const ppf_model_t* models,
                             const ppf_scene_t* scenes, float* poses_out, ppf_stats* stats_out);
 
+/* clusterPoses (src/transformation_clustering.cpp:62-123), the greedy
+ * clustering of the cpu_clustering path, on the device: poses (n row-major
+ * 4x4, host or device) sorted by votes descending (stable: equal votes keep
+ * their input order; the reference's std::sort leaves them unspecified),
+ * each joining the first cluster whose first pose is within trans_thresh and
+ * rot_thresh radians, else starting one; the (at most) three clusters with
+ * most votes, averaged (translations, and quaternions in 4-D renormalised),
+ * go to out_poses (3 x 16, host) and their vote totals to out_votes. */
+ppf_status ppf_cluster_poses(ppf_context_t ctx, const float* transforms, const uint32_t* votes, uint64_t n,
+                             float trans_thresh, float rot_thresh, float* out_poses, uint32_t* out_votes,
+                             uint32_t* n_clusters);
+
 /* pcl::io::loadPLYFile<pcl::PointNormal> as the alignment driver loads its
  * scene and model files (src/alignment.cpp:212,241): the vertex element's x,
  * y, z and nx, ny, nz (or normal_x, normal_y, normal_z), any scalar type,

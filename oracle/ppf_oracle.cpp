@@ -517,7 +517,10 @@ int orc_cluster_poses(const float* poses, const uint32_t* votes, int64_t n, floa
   };
   std::vector<PV> pv(n);
   for (int64_t i = 0; i < n; ++i) pv[i] = PV{poses + 16 * i, votes[i]};
-  std::sort(pv.begin(), pv.end(), [](const PV& a, const PV& b) { return a.votes > b.votes; });
+  // The reference sorts with std::sort (transformation_clustering.cpp:66),
+  // which leaves equal vote counts in an unspecified order; a stable sort
+  // keeps them in input order (for lookups: vote code order).
+  std::stable_sort(pv.begin(), pv.end(), [](const PV& a, const PV& b) { return a.votes > b.votes; });
   std::vector<std::vector<PV>> clusters;
   std::vector<std::pair<size_t, unsigned int>> cluster_votes;
   for (int64_t p = 0; p < n; ++p) {
@@ -535,7 +538,7 @@ int orc_cluster_poses(const float* poses, const uint32_t* votes, int64_t n, floa
       cluster_votes.push_back(std::pair<size_t, unsigned int>(clusters.size() - 1, pv[p].votes));
     }
   }
-  std::sort(cluster_votes.begin(), cluster_votes.end(),
+  std::stable_sort(cluster_votes.begin(), cluster_votes.end(),
             [](const std::pair<size_t, unsigned int>& a, const std::pair<size_t, unsigned int>& b) {
               return a.second > b.second;
             });

@@ -17,6 +17,7 @@ from .api import (  # noqa: F401
     Scene,
     Server,
     cloud_extent,
+    cluster_poses,
     ht_dist,
     load_ply,
     load_xf,

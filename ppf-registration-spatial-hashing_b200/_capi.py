@@ -88,6 +88,7 @@ SIGNATURES = {
     "ppf_model_all_votes": (C.c_int, [_vp, _vp, _u64p, _u32p, C.c_uint64, _u64p]),
     "ppf_model_pair_vote_counts": (C.c_int, [_vp, _vp, _vp]),
     "ppf_lookup_batch": (C.c_int, [_vp, C.c_uint64, _vp, _vp, _vp, _vp]),
+    "ppf_cluster_poses": (C.c_int, [_vp, _vp, _vp, C.c_uint64, C.c_float, C.c_float, _vp, _vp, _vp]),
     "ppf_ply_read": (C.c_int, [C.c_char_p, _vp, _vp, C.c_uint64, _u64p]),
     "ppf_ply_write": (C.c_int, [C.c_char_p, _vp, _vp, C.c_uint64]),
     "ppf_cloud_extent": (C.c_int, [_vp, _vp, C.c_uint64, _vp, _vp]),

@@ -319,6 +319,23 @@ def pair_keys(cloud, d_dist: float, ref_point_downsample_factor: int = 1, contex
     return out.reshape(bp.n, bp.n)
 
 
+def cluster_poses(transforms, votes, trans_thresh: float, rot_thresh: float, context=None):
+    """clusterPoses (src/transformation_clustering.cpp:62-123) on the device:
+    (poses (k, 4, 4), vote totals (k,)) of the k <= 3 best greedy clusters."""
+    ctx = context or default_context()
+    T = np.ascontiguousarray(np.asarray(transforms, np.float32).reshape(-1, 16))
+    v = np.ascontiguousarray(np.asarray(votes, np.uint32))
+    if len(T) != len(v):
+        raise ValueError("one vote count per pose is required")
+    out = np.zeros((3, 16), np.float32)
+    ov = np.zeros(3, np.uint32)
+    nc = C.c_uint32()
+    _check(_lib().ppf_cluster_poses(ctx.handle, C.c_void_p(T.ctypes.data), C.c_void_p(v.ctypes.data), len(v),
+                                    float(trans_thresh), float(rot_thresh), C.c_void_p(out.ctypes.data),
+                                    C.c_void_p(ov.ctypes.data), C.byref(nc)))
+    return out[: nc.value].reshape(-1, 4, 4), ov[: nc.value]
+
+
 def load_ply(path):
     """pcl::io::loadPLYFile<PointNormal> as the alignment driver uses it
     (src/alignment.cpp:212,241): (points, normals) float32 (n, 3)."""

@@ -101,14 +101,20 @@ LookupOut finish_lookup(Context& ctx, Model& m, LookupState& st, const SceneData
   }
   compute_poses(ctx, m, s, st);
   if (m.cpu_clustering) {
-    std::vector<float> T(U * 16);
-    std::vector<uint32_t> cnt(U);
-    PPF_CUDA(cudaMemcpyAsync(T.data(), st.transforms.ptr, U * 64, cudaMemcpyDeviceToHost, ctx.stream));
-    PPF_CUDA(cudaMemcpyAsync(cnt.data(), st.counts.ptr, U * 4, cudaMemcpyDeviceToHost, ctx.stream));
-    PPF_CUDA(cudaStreamSynchronize(ctx.stream));
     float poses[48];
     uint32_t votes[3];
-    int nc = cluster_poses_cpu(T.data(), cnt.data(), U, m.t.d_dist, PPF_D_ANGLE_HOST, poses, votes);
+    int nc = 0;
+    if (ctx.host_greedy) {
+      std::vector<float> T(U * 16);
+      std::vector<uint32_t> cnt(U);
+      PPF_CUDA(cudaMemcpyAsync(T.data(), st.transforms.ptr, U * 64, cudaMemcpyDeviceToHost, ctx.stream));
+      PPF_CUDA(cudaMemcpyAsync(cnt.data(), st.counts.ptr, U * 4, cudaMemcpyDeviceToHost, ctx.stream));
+      PPF_CUDA(cudaStreamSynchronize(ctx.stream));
+      nc = cluster_poses_cpu(T.data(), cnt.data(), U, m.t.d_dist, PPF_D_ANGLE_HOST, poses, votes);
+    } else {
+      nc = cluster_poses_greedy_gpu(ctx, st.transforms.as<float>(), st.counts.as<uint32_t>(), U, m.t.d_dist,
+                                    PPF_D_ANGLE_HOST, poses, votes);
+    }
     st.cpu_poses.assign(poses, poses + 16 * nc);
     if (nc > 0) std::memcpy(out.pose, poses, sizeof(out.pose));
     out.stats.max_idx = 0;
@@ -211,6 +217,7 @@ void init_context(Context& c, int device) {
   PPF_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device));
   c.vote_smem_limit = optin - 2048;  // static shared memory of the vote kernel
   if (const char* e = std::getenv("PPF_B200_CHECKS")) c.checks = e[0] == '1';
+  if (const char* e = std::getenv("PPF_B200_HOST_GREEDY")) c.host_greedy = e[0] == '1';
   // test hook: a small initial candidate buffer exercises its growth path
   if (const char* e = std::getenv("PPF_B200_CANDIDATE_CAP")) {
     long long v = std::atoll(e);
@@ -430,6 +437,37 @@ ppf_status ppf_voxel_downsample(ppf_context_t ctx, const float* xyz, const float
     copy_out(out_xyz, ox.ptr, K * 12, ctx->c.stream);
     copy_out(out_nxyz, on.ptr, K * 12, ctx->c.stream);
     PPF_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    return PPF_OK;
+  });
+}
+
+ppf_status ppf_cluster_poses(ppf_context_t ctx, const float* transforms, const uint32_t* votes, uint64_t n,
+                             float trans_thresh, float rot_thresh, float* out_poses, uint32_t* out_votes,
+                             uint32_t* n_clusters) {
+  return guarded([&]() {
+    PPF_REQUIRE(ctx && out_poses && out_votes && n_clusters && (n == 0 || (transforms && votes)),
+                PPF_ERR_INVALID_ARGUMENT, "null argument");
+    PPF_CUDA(cudaSetDevice(ctx->c.device));
+    StreamScope scope(ctx->c.stream);
+    DevBuf tT, tV;
+    const float* T = transforms;
+    const uint32_t* V = votes;
+    if (n && !is_device_pointer(transforms)) {
+      tT.reserve(n * 64);
+      PPF_CUDA(cudaMemcpyAsync(tT.ptr, transforms, n * 64, cudaMemcpyHostToDevice, ctx->c.stream));
+      T = tT.as<float>();
+    }
+    if (n && !is_device_pointer(votes)) {
+      tV.reserve(n * 4);
+      PPF_CUDA(cudaMemcpyAsync(tV.ptr, votes, n * 4, cudaMemcpyHostToDevice, ctx->c.stream));
+      V = tV.as<uint32_t>();
+    }
+    float p[48];
+    uint32_t v[3];
+    const int nc = cluster_poses_sorted_gpu(ctx->c, T, V, n, trans_thresh, rot_thresh, p, v);
+    std::memcpy(out_poses, p, sizeof(float) * 16 * nc);
+    std::memcpy(out_votes, v, sizeof(uint32_t) * nc);
+    *n_clusters = (uint32_t)nc;
     return PPF_OK;
   });
 }

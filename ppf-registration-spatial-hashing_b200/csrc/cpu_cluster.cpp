@@ -81,7 +81,10 @@ int cluster_poses_cpu(const float* poses, const uint32_t* votes, size_t n, float
   };
   std::vector<Item> items(n);
   for (size_t i = 0; i < n; ++i) items[i] = Item{poses + 16 * i, votes[i]};
-  std::sort(items.begin(), items.end(), [](const Item& a, const Item& b) { return a.votes > b.votes; });
+  // The reference sorts with std::sort (src/transformation_clustering.cpp:66),
+  // which leaves equal vote counts in an unspecified order; the stable sort
+  // keeps them in input order, the vote code order of the kept votes.
+  std::stable_sort(items.begin(), items.end(), [](const Item& a, const Item& b) { return a.votes > b.votes; });
   std::vector<std::vector<Item>> clusters;
   std::vector<std::pair<size_t, unsigned int>> totals;
   for (const Item& it : items) {
@@ -98,7 +101,7 @@ int cluster_poses_cpu(const float* poses, const uint32_t* votes, size_t n, float
       totals.emplace_back(clusters.size() - 1, it.votes);
     }
   }
-  std::sort(totals.begin(), totals.end(),
+  std::stable_sort(totals.begin(), totals.end(),
             [](const std::pair<size_t, unsigned int>& a, const std::pair<size_t, unsigned int>& b) {
               return a.second > b.second;
             });

@@ -50,6 +50,7 @@ struct Context {
   int vote_smem_limit = 0;  // max dynamic shared memory per vote block
   size_t launches = 0;      // kernels launched (running total)
   bool checks = false;      // self-checking kernels (PPF_B200_CHECKS=1)
+  bool host_greedy = false; // cpu_clustering on the host (PPF_B200_HOST_GREEDY=1)
   ~Context();
 };
 
@@ -207,6 +208,13 @@ uint64_t server_submit(Server* srv, const float* xyz, const float* nxyz, uint64_
 ppf_status server_wait(Server* srv, uint64_t ticket, float* poses, ppf_stats* stats, double* latency_ms,
                        std::string* error);
 void server_destroy(Server* srv);
+
+// ---- greedy clustering of the cpu_clustering path on the device (greedy.cu)
+int cluster_poses_greedy_gpu(Context& ctx, const float* transforms_dev, const uint32_t* votes_dev, size_t U,
+                             float trans_thresh, float rot_thresh, float out_poses[3 * 16], uint32_t out_votes[3]);
+
+int cluster_poses_sorted_gpu(Context& ctx, const float* transforms_dev, const uint32_t* votes_dev, size_t U,
+                             float trans_thresh, float rot_thresh, float out_poses[3 * 16], uint32_t out_votes[3]);
 
 // ---- greedy CPU clustering (cpu_cluster.cpp)
 int cluster_poses_cpu(const float* poses, const uint32_t* votes, size_t n, float trans_thresh,

@@ -305,3 +305,52 @@ def test_candidate_buffer_growth(pkg, ctx, monkeypatch):
     codes, counts = M.get_votes()
     assert np.array_equal(codes, codes_ref) and np.array_equal(counts, counts_ref)
     assert _same(pose, pose_ref)
+
+
+def test_gpu_greedy_clustering_equals_host(pkg, ctx, oracle, monkeypatch):
+    """cpu_clustering=True runs the greedy clustering on the device; its best
+    pose and vote total equal the host restatement's on the same kept votes."""
+    thr = 0.3
+    spec = pkg.synthetic.config_plain(seed=141, n_model=1200, n_plane=2500, n_box=800)
+    m, s, d = spec.models[0], spec.scene, spec.d_dists[0]
+    model = pkg.Model(m, d, thr, cpu_clustering=True, context=ctx)
+    scene = pkg.Scene(s, d, 5, context=ctx)
+    pose = model.ppf_lookup(scene).copy()
+    T = model.getTransformations()
+    _, counts = model.get_votes()
+    out, votes = oracle.cluster_poses(T, counts, d, 2 * np.float32(np.pi) / 30)
+    assert np.array_equal(pose, out[0])
+    assert model.stats["best_score"] == float(votes[0])
+    monkeypatch.setenv("PPF_B200_HOST_GREEDY", "1")
+    hctx = pkg.Context(0)
+    hm = pkg.Model(m, d, thr, cpu_clustering=True, context=hctx)
+    assert np.array_equal(hm.ppf_lookup(pkg.Scene(s, d, 5, context=hctx)), pose)
+
+
+def test_gpu_greedy_clustering_many_poses(pkg, ctx, oracle):
+    """The device clusterPoses across several 16384-pose chunks equals the
+    host restatement: 40,000 noisy poses around 200 centres, votes 1..50."""
+    rng = np.random.default_rng(151)
+    centres = []
+    for _ in range(200):
+        q = rng.normal(size=4)
+        q /= np.linalg.norm(q)
+        w, x, y, z = q
+        R = np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+                      [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+                      [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
+        centres.append((R, rng.uniform(-0.3, 0.3, 3)))
+    T = np.zeros((40000, 4, 4), np.float32)
+    for i in range(40000):
+        R, t = centres[rng.integers(200)]
+        a = rng.normal(size=3) * 0.02
+        K = np.array([[0, -a[2], a[1]], [a[2], 0, -a[0]], [-a[1], a[0], 0]])
+        T[i, :3, :3] = R @ (np.eye(3) + K + 0.5 * K @ K)
+        T[i, :3, 3] = t + rng.normal(size=3) * 0.002
+        T[i, 3, 3] = 1
+    votes = rng.integers(1, 51, 40000).astype(np.uint32)
+    d, rot = 0.01, 2 * np.float32(np.pi) / 30
+    gp, gv = pkg.cluster_poses(T, votes, d, rot, context=ctx)
+    hp, hv = oracle.cluster_poses(T, votes, d, rot)
+    assert np.array_equal(gv, hv)
+    assert np.array_equal(gp, hp)
