@@ -77,8 +77,12 @@ LookupOut finish_lookup(Context& ctx, Model& m, LookupState& st, const SceneData
                         const unsigned long long* cand_code, const uint32_t* cand_count,
                         size_t launches0, bool own_state) {
   LookupOut out;
-  if (own_state) m.cand_hint = vr.n_cand;
-  ctx.cand_hints[model_signature(m)] = vr.n_cand;
+  // After an overflow the recounted items emit against a higher running
+  // maximum, so the cells the first launch asked for are the better size.
+  const size_t hint = std::max<size_t>(vr.n_cand, vr.n_needed);
+  if (own_state) m.cand_hint = hint;
+  ctx.cand_hints[model_signature(m)] = hint;
+  out.cand_hint = hint;
   st.U = 0;
   out.stats.n_votes = vr.n_votes;
   out.stats.n_matched_pairs = vr.n_matched;

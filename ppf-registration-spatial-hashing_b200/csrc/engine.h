@@ -136,6 +136,7 @@ struct VoteResult {
   uint64_t n_votes = 0, n_matched = 0, n_exact = 0;
   uint64_t n_cand = 0;
   uint32_t n_redo = 0;  // items emitted by a second launch after the buffer grew
+  uint64_t n_needed = 0;  // cells the first launch's items asked for (sizes the next buffer)
   float vote_ms = 0;
 };
 // Runs the vote pass.  emit_all: emit every nonzero cell (no threshold);
@@ -190,6 +191,7 @@ struct LookupOut {
   ppf_status status = PPF_OK;
   float pose[16] = {0};
   ppf_stats stats{};
+  size_t cand_hint = 0;  // candidate cells to provide for the next pass of this model
 };
 void init_context(Context& c, int device);
 // Lookups of (models[i], scenes[i]) with one batched vote pass.  states:

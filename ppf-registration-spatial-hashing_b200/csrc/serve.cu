@@ -109,7 +109,7 @@ struct Server {
         std::memcpy(&r->poses[16 * t], out[k].pose, sizeof(out[k].pose));
         r->stats[t] = out[k].stats;
         if (out[k].status != PPF_OK) r->status = out[k].status;
-        hints[r->targets[t]] = out[k].stats.n_candidates;
+        hints[r->targets[t]] = out[k].cand_hint;
       }
     }
   }

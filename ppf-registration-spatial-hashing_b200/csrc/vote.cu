@@ -641,6 +641,7 @@ VoteResult run_votes(Context& ctx, const Model& m, const SceneData& s, bool emit
     // what every item asked for, then count those items again.
     unsigned long long needed;
     memcpy(&needed, h + 10, sizeof(needed));
+    r.n_needed = needed;
     const size_t want = std::max<size_t>(needed, 2 * ctx.cand_cap);
     PPF_REQUIRE(want < 0xffffffffull, PPF_ERR_OUT_OF_MEMORY, "more than 2^32 vote candidates");
     DevBuf nc, nn, items;
@@ -779,6 +780,7 @@ void run_votes_batch(Context& ctx, std::vector<BatchVote>& reqs) {
     if (!hc[3]) continue;
     unsigned long long needed;
     memcpy(&needed, hc + 10, sizeof(needed));
+    reqs[i].r.n_needed = needed;
     const size_t want = std::max<size_t>(needed, 2 * reqs[i].cap);
     PPF_REQUIRE(want < 0xffffffffull, PPF_ERR_OUT_OF_MEMORY, "more than 2^32 vote candidates");
     DevBuf nc, nn, items;
