@@ -185,9 +185,10 @@ def run_reference_arm(args):
         return
     _, spec = workload()
     t0 = time.perf_counter()
-    # each step: a bounded sample (2 reference points per model, model builds in
-    # full); the host path needs no warm-up, so the W warm-up steps are not run
-    samples = [cpu_baseline(spec, sample_refs=2) for _ in range(max(1, args.steps))]
+    # each step: the cpu_baseline sample (about 6 reference points per model,
+    # model builds in full, 20-40 s); the host path needs no warm-up, so the W
+    # warm-up steps are not run
+    samples = [cpu_baseline(spec, sample_refs=args.cpu_refs) for _ in range(max(1, args.steps))]
     cb = dict(samples[len(samples) // 2])
     cb["value"] = statistics.median(s["value"] for s in samples)
     cb["sample"] = f"median of {len(samples)} steps, each: " + cb["sample"]
