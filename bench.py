@@ -262,7 +262,7 @@ def run_serve(args):
     ctx.synchronize()
     t_batch = time.perf_counter() - t0
 
-    srv = pkg.Server(lib, workers=2, max_batch=16)
+    srv = pkg.Server(lib, workers=args.serve_workers, max_batch=args.serve_max_batch)
     for t in [srv.submit(sc, ids, REF_DF) for sc, ids in reqs[:4]]:
         srv.wait(t, raise_on_no_votes=False)
 
@@ -304,7 +304,8 @@ def run_serve(args):
                                    f"pts, tau_d=0.04), {len(reqs)} scenes of {args.serve_scene_range[0]}-"
                                    f"{args.serve_scene_range[1]} pts holding 1-4 models each, ref_point_df=5, "
                                    "threshold 0.3",
-                       "served": "2 workers, max_batch 16, Poisson arrivals at 70% and 150% of the batched rate"}}
+                       "served": f"{args.serve_workers} workers, max_batch {args.serve_max_batch}, Poisson arrivals "
+                                 "at 70% and 150% of the batched rate"}}
     print(json.dumps(line), flush=True)
 
 
@@ -353,6 +354,8 @@ def main():
     ap.add_argument("--serve-scenes", type=int, default=64)
     ap.add_argument("--serve-model-range", type=int, nargs=2, default=(2000, 6000))
     ap.add_argument("--serve-scene-range", type=int, nargs=2, default=(5000, 40000))
+    ap.add_argument("--serve-workers", type=int, default=4)
+    ap.add_argument("--serve-max-batch", type=int, default=16)
     ap.add_argument("--profile-case", action="store_true",
                     help="one lookup of one model at ref_point_df=50 (short vote launch for ncu)")
     ap.add_argument("--profile-model", type=int, default=0)
@@ -388,7 +391,7 @@ def main():
         with torch.cuda.stream(stream):
             flush.fill_(1)
 
-    for _ in range(args.warmup):
+    for _ in range(max(1, args.warmup)):  # at least one, for the correctness guard below
         poses, stats = step(models_d, scene_d)
         flush_l2()
     # correctness guard of the measured configuration

@@ -469,7 +469,7 @@ class Server:
     same (model, scene).  Submissions and waits may come from several threads.
     """
 
-    def __init__(self, models, memory_budget: int = 40 << 30, workers: int = 2, max_batch: int = 16,
+    def __init__(self, models, memory_budget: int = 40 << 30, workers: int = 4, max_batch: int = 16,
                  device: int = 0):
         self.models = list(models)
         arr = (C.c_void_p * len(self.models))(*[m.handle for m in self.models])

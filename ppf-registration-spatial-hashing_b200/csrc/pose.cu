@@ -368,23 +368,44 @@ __global__ void __launch_bounds__(kClusterTile) cluster_tiled_kernel(TiledArgs a
           }
           uint32_t mask = __ballot_sync(0xffffffffu, in);
           while (mask) {
-            const uint32_t jj = j0 + (uint32_t)(__ffs(mask) - 1);
-            mask &= mask - 1;
+            // up to 2 marked sources at a time: their tests are independent,
+            // their weights are added in ascending order as before
+            uint32_t jj[2];
+            int nj = 0;
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+              jj[u] = j0 + (mask ? (uint32_t)(__ffs(mask) - 1) : 0u);
+              nj += mask ? 1 : 0;
+              mask &= mask - 1;
+            }
             if (!valid) continue;
-            const float qd = fabsf(8 * (1 - dot4(q, sq[jj])));
-            if (qd < rot_sq) {
-              const float4 sj = stw[jj];
-              const float3 tj = make_float3(sj.x, sj.y, sj.z);
+            float4 sqv[2], swv[2];
+            bool pass[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+              sqv[u] = sq[jj[u]];
+              swv[u] = stw[jj[u]];
+            }
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+              const float qd = fabsf(8 * (1 - dot4(q, sqv[u])));
+              bool ok = u < nj && qd < rot_sq;
               if (!a.use_l1) {
-                float nd = norm3(v3_sub(t, tj));
-                if (!(nd < a.d_dist)) continue;
+                const float nd = norm3(v3_sub(t, make_float3(swv[u].x, swv[u].y, swv[u].z)));
+                ok = ok && nd < a.d_dist;
               }
+              pass[u] = ok;
+            }
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+              if (!pass[u]) continue;
+              const float3 tj = make_float3(swv[u].x, swv[u].y, swv[u].z);
               if (a.use_avg) {
                 to = v3_scale(c, to);
-                to = v3_add(to, v3_scale(sj.w, tj));
-                to = v3_scale(1 / (c + sj.w), to);
+                to = v3_add(to, v3_scale(swv[u].w, tj));
+                to = v3_scale(1 / (c + swv[u].w), to);
               }
-              c += sj.w;
+              c += swv[u].w;
             }
           }
         }
