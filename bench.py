@@ -101,11 +101,13 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index, interval_ms=2500):
+    def __init__(self, gpu_index, interval_ms=2500, out_dir=None):
+        import tempfile
+
         self.gpu = gpu_index
         self.interval_ms = int(interval_ms)
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_rank{gpu_index}.csv"
+        self.path = Path(out_dir or tempfile.gettempdir()) / f"clocks_rank{gpu_index}.csv"
 
     def __enter__(self):
         try:
@@ -345,6 +347,7 @@ def main():
     ap.add_argument("--cpu-refs", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--clocks-dir", default=None, help="where the clock samples are written (default: temp dir)")
     ap.add_argument("--clock-interval-ms", type=int, default=2500,
                     help="nvidia-smi sampling interval during the timed region (each query stalls the "
                          "engine's CUDA calls briefly)")
@@ -411,7 +414,7 @@ def main():
     votes = 0
     traffic = 0.0
     pairs = 0
-    with ClockSampler(local, args.clock_interval_ms) as clk:
+    with ClockSampler(local, args.clock_interval_ms, args.clocks_dir) as clk:
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
