@@ -467,6 +467,8 @@ def main():
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(len(spec.models) * 64)}
 
     if rank != 0:
+        if dist:
+            dist.destroy_process_group()
         return
     peak, peak_kind = measured_peaks()
     alg_bytes = 4.0 * votes + 32.0 * pairs
