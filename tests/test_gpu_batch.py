@@ -96,3 +96,20 @@ def test_registration_scenes_by_models_equals_lookups(pkg, ctx, library):
             assert np.array_equal(poses[i][j], pose), (i, j)
             assert stats[i][j]["n_votes"] == model.stats["n_votes"]
             assert stats[i][j]["n_kept"] == model.stats["n_kept"]
+
+
+def test_batch_modes_equal_single_lookups(pkg, ctx, library):
+    """L1, averaged-cluster and greedy (cpu_clustering) models in one batch:
+    each request equals its single lookup."""
+    specs, _, scenes = library
+    sp = specs[1]
+    d = sp.d_dists[0]
+    kinds = [dict(use_l1_norm=True), dict(use_averaged_clusters=True), dict(cpu_clustering=True), {}]
+    models = [pkg.Model(sp.models[0], d, sp.vote_count_threshold, context=ctx, **kw) for kw in kinds]
+    scene = pkg.Scene(sp.scene, d, sp.ref_point_df, context=ctx)
+    poses, stats = pkg.lookup_batch(models, [scene] * len(models), context=ctx, return_stats=True)
+    for j, m in enumerate(models):
+        pose, st, _, _ = _alone(m, scene)
+        assert np.array_equal(poses[j], pose), kinds[j]
+        for k in KEYS:
+            assert stats[j][k] == st[k], (kinds[j], k)
