@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define PPF_B200_ABI_VERSION 1
+#define PPF_B200_ABI_VERSION 2
 
 typedef enum ppf_status {
   PPF_OK = 0,
@@ -57,6 +57,8 @@ typedef struct ppf_stats {
   float total_ms;            /* device time of the whole lookup */
   uint32_t gpu_launches;     /* kernels launched by the lookup */
   uint32_t n_redo_items;     /* vote items emitted again after the candidate buffer grew */
+  uint32_t cluster_path;     /* clustering that ran: 0 none, 1 ordered sums per cell tile,
+                                2 per-pose neighbour lists, 3 split exact sums, 4 greedy */
 } ppf_stats;
 
 /* Error text of the last failing call on this thread ("" if none). */

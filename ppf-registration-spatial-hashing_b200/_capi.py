@@ -38,6 +38,7 @@ class ppf_stats(C.Structure):
         ("total_ms", C.c_float),
         ("gpu_launches", C.c_uint32),
         ("n_redo_items", C.c_uint32),
+        ("cluster_path", C.c_uint32),
     ]
 
     def as_dict(self):

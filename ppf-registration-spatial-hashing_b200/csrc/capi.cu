@@ -123,12 +123,14 @@ LookupOut finish_lookup(Context& ctx, Model& m, LookupState& st, const SceneData
     if (nc > 0) std::memcpy(out.pose, poses, sizeof(out.pose));
     out.stats.max_idx = 0;
     out.stats.best_score = nc > 0 ? (float)votes[0] : 0.f;
+    out.stats.cluster_path = 4;
   } else {
     float best_score = 0;
     size_t idx = cluster_poses_gpu(ctx, m, st, &best_score);
     PPF_CUDA(cudaMemcpyAsync(out.pose, st.best.ptr, sizeof(out.pose), cudaMemcpyDeviceToHost, ctx.stream));
     out.stats.max_idx = idx;
     out.stats.best_score = best_score;
+    out.stats.cluster_path = st.cluster_path;
   }
   PPF_CUDA(cudaEventRecord(ctx.ev[3], ctx.stream));
   PPF_CUDA(cudaStreamSynchronize(ctx.stream));
@@ -222,6 +224,7 @@ void init_context(Context& c, int device) {
   c.vote_smem_limit = optin - 2048;  // static shared memory of the vote kernel
   if (const char* e = std::getenv("PPF_B200_CHECKS")) c.checks = e[0] == '1';
   if (const char* e = std::getenv("PPF_B200_HOST_GREEDY")) c.host_greedy = e[0] == '1';
+  if (const char* e = std::getenv("PPF_B200_CLUSTER_SPLIT")) c.cluster_split = e[0] != '0';
   // test hook: a small initial candidate buffer exercises its growth path
   if (const char* e = std::getenv("PPF_B200_CANDIDATE_CAP")) {
     long long v = std::atoll(e);

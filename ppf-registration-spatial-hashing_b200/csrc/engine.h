@@ -51,6 +51,7 @@ struct Context {
   size_t launches = 0;      // kernels launched (running total)
   bool checks = false;      // self-checking kernels (PPF_B200_CHECKS=1)
   bool host_greedy = false; // cpu_clustering on the host (PPF_B200_HOST_GREEDY=1)
+  bool cluster_split = true; // exact-sum split clustering allowed (PPF_B200_CLUSTER_SPLIT=0: never)
   ~Context();
 };
 
@@ -105,9 +106,11 @@ struct LookupState {
   DevBuf cells_sorted, cells_map, cells_uniq, cells_first, cells_count;
   DevBuf cells3;      // int4 U: integer cell of each pose
   DevBuf qs, tws, adjrun, item_off;  // cell-major clustering tables
+  DevBuf item_off32;  // split clustering: (32-target tile, neighbour) items per run
   DevBuf tmp64, tmp32a, tmp32b, perm;
   DevBuf tperm;       // clustering target order (cell, rotation bucket)
   DevBuf best;        // float[16] pose + int idx
+  uint32_t cluster_path = 0;  // ppf_stats::cluster_path of the last clustering
   std::vector<float> cpu_poses;
 };
 

@@ -236,12 +236,14 @@ __global__ void target_keys_kernel(const uint32_t* __restrict__ sorted_keys, con
     keys[p] = ((unsigned long long)sorted_keys[p] << 16) | quat_bucket(qs[p]);
 }
 
-// Per cell run: its 27 neighbour runs (-1: none / the centre) and the number
-// of target tiles.
+// Per cell run: its 27 neighbour runs (-1: none / the centre), the number of
+// target tiles and, if items32 is set, the number of split items (32-target
+// tiles x 27 neighbours).
 __global__ void run_adjacency_kernel(const uint32_t* __restrict__ first, const uint32_t* __restrict__ count,
                                      size_t Kc, const uint32_t* __restrict__ map,
                                      const int4* __restrict__ cells3, const uint32_t* __restrict__ uniq,
-                                     int* __restrict__ adjrun, uint32_t* __restrict__ tiles) {
+                                     int* __restrict__ adjrun, uint32_t* __restrict__ tiles,
+                                     uint32_t* __restrict__ items32) {
   for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < Kc;
        r += (size_t)gridDim.x * blockDim.x) {
     const uint32_t f = first[r], n = count[r];
@@ -264,6 +266,7 @@ __global__ void run_adjacency_kernel(const uint32_t* __restrict__ first, const u
           adjrun[r * 27 + b] = run;
         }
     tiles[r] = (n + kClusterTile - 1) / kClusterTile;
+    if (items32) items32[r] = (n + 31) / 32 * 27;
   }
 }
 
@@ -421,6 +424,118 @@ __global__ void __launch_bounds__(kClusterTile) cluster_tiled_kernel(TiledArgs a
   }
 }
 
+// ---- split clustering (exact sums) ----------------------------------------
+// When every weight is an integer and the weights' absolute sum is below
+// 2^24, every partial score is an integer that a float holds exactly, so a
+// target's score is the same whatever the order of its additions.  The work
+// can then be split per (32-target tile, neighbour cell): each warp tests one
+// neighbour cell's poses against its 32 targets, in the same box-filtered way
+// as cluster_tiled_kernel, and adds its partial sum with a float atomic.  A
+// lookup with few poses then spreads over up to 27x more warps.
+
+// nonint: some weight is not an integer below 2^24 (or is NaN); abs_sum: the
+// sum of |weight| over all poses.
+__global__ void weight_check_kernel(const float* __restrict__ w, size_t U, uint32_t* __restrict__ nonint,
+                                    unsigned long long* __restrict__ abs_sum) {
+  unsigned long long s = 0;
+  bool bad = false;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < U; i += (size_t)gridDim.x * blockDim.x) {
+    const float x = w[i], ax = fabsf(x);
+    if (!(ax < 16777216.f) || x != truncf(x)) bad = true;
+    else s += (unsigned long long)ax;
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  bad = __any_sync(0xffffffffu, bad);
+  if ((threadIdx.x & 31) == 0) {
+    if (bad) atomicOr(nonint, 1u);
+    if (s) atomicAdd(abs_sum, s);
+  }
+}
+
+// Scores start at 1 (the pose itself); translations stay the snapshot's.
+__global__ void split_init_kernel(size_t U, const float* __restrict__ trans0, float* __restrict__ scores,
+                                  float* __restrict__ trans) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < U; i += (size_t)gridDim.x * blockDim.x) {
+    scores[i] = 1.f;
+    trans[3 * i] = trans0[3 * i];
+    trans[3 * i + 1] = trans0[3 * i + 1];
+    trans[3 * i + 2] = trans0[3 * i + 2];
+  }
+}
+
+constexpr int kSplitBlock = 256;
+
+__global__ void __launch_bounds__(kSplitBlock) cluster_split_kernel(TiledArgs a) {
+  const float rot_sq = PPF_ROT_THRESH * PPF_ROT_THRESH;
+  const int lane = threadIdx.x & 31;
+  constexpr float kQuatMargin = 0.25f;  // as cluster_tiled_kernel
+  const float t_margin = a.use_l1 ? INFINITY : a.d_dist * 1.0001f + 1e-6f;
+  const uint32_t n_warps = gridDim.x * (kSplitBlock / 32);
+  for (uint32_t item = blockIdx.x * (kSplitBlock / 32) + (threadIdx.x >> 5); item < a.n_items;
+       item += n_warps) {
+    size_t lo = 0, hi = a.Kc;  // run r with item_off[r] <= item < item_off[r + 1]
+    while (hi - lo > 1) {
+      size_t mid = (lo + hi) >> 1;
+      if (a.item_off[mid] <= item) lo = mid;
+      else hi = mid;
+    }
+    const size_t r = lo;
+    const uint32_t k = item - a.item_off[r];
+    const int nr = a.adjrun[r * 27 + k % 27];
+    if (nr < 0) continue;  // uniform over the warp
+    const uint32_t slot = a.first[r] + (k / 27) * 32 + lane;
+    const bool valid = slot < a.first[r] + a.count[r];
+    const uint32_t p = valid ? a.tperm[slot] : 0u;
+    float4 q = make_float4(0, 0, 0, 0), tw = make_float4(0, 0, 0, 0);
+    if (valid) {
+      q = a.qs[p];
+      tw = a.tws[p];
+    }
+    const float3 t = make_float3(tw.x, tw.y, tw.z);
+    const float4 qlo = make_float4(warp_min(valid ? q.x : INFINITY) - kQuatMargin,
+                                   warp_min(valid ? q.y : INFINITY) - kQuatMargin,
+                                   warp_min(valid ? q.z : INFINITY) - kQuatMargin,
+                                   warp_min(valid ? q.w : INFINITY) - kQuatMargin);
+    const float4 qhi = make_float4(warp_max(valid ? q.x : -INFINITY) + kQuatMargin,
+                                   warp_max(valid ? q.y : -INFINITY) + kQuatMargin,
+                                   warp_max(valid ? q.z : -INFINITY) + kQuatMargin,
+                                   warp_max(valid ? q.w : -INFINITY) + kQuatMargin);
+    const float3 tlo = make_float3(warp_min(valid ? t.x : INFINITY) - t_margin,
+                                   warp_min(valid ? t.y : INFINITY) - t_margin,
+                                   warp_min(valid ? t.z : INFINITY) - t_margin);
+    const float3 thi = make_float3(warp_max(valid ? t.x : -INFINITY) + t_margin,
+                                   warp_max(valid ? t.y : -INFINITY) + t_margin,
+                                   warp_max(valid ? t.z : -INFINITY) + t_margin);
+    const uint32_t f = a.first[nr], n = a.count[nr];
+    float c = 0;
+    for (uint32_t j0 = 0; j0 < n; j0 += 32) {
+      float4 sj = make_float4(0, 0, 0, 0), wj = make_float4(0, 0, 0, 0);
+      bool in = false;
+      if (j0 + lane < n) {
+        sj = a.qs[f + j0 + lane];
+        wj = a.tws[f + j0 + lane];
+        in = sj.x >= qlo.x && sj.x <= qhi.x && sj.y >= qlo.y && sj.y <= qhi.y && sj.z >= qlo.z &&
+             sj.z <= qhi.z && sj.w >= qlo.w && sj.w <= qhi.w && wj.x >= tlo.x && wj.x <= thi.x &&
+             wj.y >= tlo.y && wj.y <= thi.y && wj.z >= tlo.z && wj.z <= thi.z;
+      }
+      uint32_t mask = __ballot_sync(0xffffffffu, in);
+      while (mask) {
+        const int src = __ffs(mask) - 1;
+        mask &= mask - 1;
+        const float4 s = make_float4(__shfl_sync(0xffffffffu, sj.x, src), __shfl_sync(0xffffffffu, sj.y, src),
+                                     __shfl_sync(0xffffffffu, sj.z, src), __shfl_sync(0xffffffffu, sj.w, src));
+        const float4 sw = make_float4(__shfl_sync(0xffffffffu, wj.x, src), __shfl_sync(0xffffffffu, wj.y, src),
+                                      __shfl_sync(0xffffffffu, wj.z, src), __shfl_sync(0xffffffffu, wj.w, src));
+        bool ok = valid && fabsf(8 * (1 - dot4(q, s))) < rot_sq;
+        if (!a.use_l1) ok = ok && norm3(v3_sub(t, make_float3(sw.x, sw.y, sw.z))) < a.d_dist;
+        if (ok) c += sw.w;
+      }
+    }
+    if (valid && c != 0.f) atomicAdd(&a.scores[a.map[p]], c);
+  }
+}
+
 // First index of the largest score (thrust::max_element semantics), then the
 // pose assembly of ppf.cu:78-93 into best[0..15]; best[16] = score and
 // best[18..19] = index (uint64).
@@ -570,6 +685,7 @@ size_t cluster_poses_gpu(Context& ctx, const Model& m, LookupState& st, float* b
   const size_t U = st.U;
   cudaStream_t stream = ctx.stream;
   float* best = grow<float>(st.best, 32);
+  st.cluster_path = 0;
   if (U <= 1) {
     PPF_CUDA(cudaMemsetAsync(best, 0, 32 * sizeof(float), stream));
     *best_score = 0;
@@ -609,18 +725,62 @@ size_t cluster_poses_gpu(Context& ctx, const Model& m, LookupState& st, float* b
   float4* tws = grow<float4>(st.tws, U);
   int* adjrun = grow<int>(st.adjrun, Kc * 27);
   uint32_t* item_off = grow<uint32_t>(st.item_off, Kc + 1);
-  PPF_CUDA(cudaMemsetAsync(ctx.counters.ptr, 0, 8, stream));
+  // Without running averages the score sums may be split across warps when
+  // they are exact in any order (integer weights, absolute sum below 2^24).
+  const bool may_split = ctx.cluster_split && !m.use_averaged_clusters;
+  uint32_t* item_off32 = may_split ? grow<uint32_t>(st.item_off32, Kc + 1) : nullptr;
+  // counters: [0] mixed cells, [1] tiles, [2] split items, [3] non-integer
+  // weight, [4..5] sum of |weight|
+  PPF_CUDA(cudaMemsetAsync(ctx.counters.ptr, 0, 24, stream));
   uint32_t* mixed = ctx.counters.as<uint32_t>();
   gather_sorted_kernel<<<grid_for(U, 256), 256, 0, stream>>>(map, U, a.quats, a.trans0, a.weighted, qs, tws);
   mixed_cells_kernel<<<grid_for(U, 256), 256, 0, stream>>>(ck, map, st.cells3.as<int4>(), U, mixed);
   run_adjacency_kernel<<<grid_for(Kc, 128), 128, 0, stream>>>(fi, ct, Kc, map, st.cells3.as<int4>(), uq,
-                                                              adjrun, item_off);
+                                                              adjrun, item_off, item_off32);
   exclusive_scan_small(item_off, Kc, mixed + 1, stream);
-  uint32_t hc[2];
-  PPF_CUDA(cudaMemcpyAsync(hc, mixed, 8, cudaMemcpyDeviceToHost, stream));
-  PPF_CUDA(cudaStreamSynchronize(stream));
   ctx.launches += 4;
-  if (hc[0]) {
+  if (may_split) {
+    exclusive_scan_small(item_off32, Kc, mixed + 2, stream);
+    weight_check_kernel<<<grid_for(U, 256), 256, 0, stream>>>(a.weighted, U, mixed + 3,
+                                                              reinterpret_cast<unsigned long long*>(mixed + 4));
+    ctx.launches += 2;
+  }
+  uint32_t hc[6];
+  PPF_CUDA(cudaMemcpyAsync(hc, mixed, sizeof(hc), cudaMemcpyDeviceToHost, stream));
+  PPF_CUDA(cudaStreamSynchronize(stream));
+  const unsigned long long abs_sum = hc[4] | ((unsigned long long)hc[5] << 32);
+  const bool split = may_split && !hc[0] && !hc[3] && abs_sum < (1ull << 24) - 1;
+  st.cluster_path = split ? 3 : hc[0] ? 2 : 1;
+  if (split) {
+    // targets of each cell ordered by rotation bucket, as below
+    unsigned long long* tkeys = grow<unsigned long long>(st.tmp64, U);
+    uint32_t* tperm = grow<uint32_t>(st.tperm, U);
+    target_keys_kernel<<<grid_for(U, 256), 256, 0, stream>>>(ck, qs, U, tkeys);
+    const size_t l1 = ctx.sort64.launches();
+    ctx.sort64.sort(tkeys, tperm, true, U, 0, 48, stream, ctx.flags.as<uint32_t>());
+    ctx.launches += 1 + ctx.sort64.launches() - l1;
+    split_init_kernel<<<grid_for(U, 256), 256, 0, stream>>>(U, a.trans0, a.scores, a.trans);
+    TiledArgs ta;
+    ta.tperm = tperm;
+    ta.first = fi;
+    ta.count = ct;
+    ta.map = map;
+    ta.adjrun = adjrun;
+    ta.item_off = item_off32;
+    ta.Kc = Kc;
+    ta.n_items = hc[2];
+    ta.qs = qs;
+    ta.tws = tws;
+    ta.d_dist = m.t.d_dist;
+    ta.use_l1 = m.use_l1_norm;
+    ta.use_avg = 0;
+    ta.scores = a.scores;
+    ta.trans = a.trans;
+    const size_t blocks = (hc[2] + kSplitBlock / 32 - 1) / (kSplitBlock / 32);
+    const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>(blocks, (size_t)sm_count() * 8));
+    cluster_split_kernel<<<grid, kSplitBlock, 0, stream>>>(ta);
+    ctx.launches += 2;
+  } else if (hc[0]) {
     cluster_kernel<<<grid_for(U, 128), 128, 0, stream>>>(a);
   } else {
     // targets of each cell ordered by rotation bucket

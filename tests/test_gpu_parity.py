@@ -354,3 +354,43 @@ def test_gpu_greedy_clustering_many_poses(pkg, ctx, oracle):
     hp, hv = oracle.cluster_poses(T, votes, d, rot)
     assert np.array_equal(gv, hv)
     assert np.array_equal(gp, hp)
+
+
+def test_split_clustering_equals_ordered(pkg, ctx, ref_gpu, monkeypatch):
+    """Integer weights with a small total take the split clustering (partial
+    sums per neighbour cell, added atomically); scores, translations, best
+    index and pose equal the ordered per-target sums and the reference's."""
+    spec = pkg.synthetic.config_plain(seed=161, n_model=900, n_plane=1800, n_box=600)
+    m, s, d = spec.models[0], spec.scene, spec.d_dists[0]
+    monkeypatch.setenv("PPF_B200_CLUSTER_SPLIT", "0")
+    octx = pkg.Context(0)
+    for kw in ({}, {"use_l1_norm": True}):
+        a = pkg.Model(m, d, 0.3, context=ctx, **kw)
+        pa = a.ppf_lookup(pkg.Scene(s, d, 5, context=ctx)).copy()
+        assert a.stats["cluster_path"] == 3, kw
+        b = pkg.Model(m, d, 0.3, context=octx, **kw)
+        pb = b.ppf_lookup(pkg.Scene(s, d, 5, context=octx)).copy()
+        assert b.stats["cluster_path"] == 1, kw
+        for x, y in zip(a.get_cluster_state(), b.get_cluster_state()):
+            assert _same(x, y), kw
+        assert a.stats["max_idx"] == b.stats["max_idx"]
+        assert _same(pa.ravel(), pb.ravel())
+        R = ref_gpu.lookup((m.points, m.normals), (s.points, s.normals), d, 5, 0.3, **kw)
+        assert _same(a.get_cluster_state()[2], R["scores"])
+        assert _same(pa.ravel(), R["pose"].ravel())
+
+
+def test_cluster_path_selection(pkg, ctx):
+    """Non-integer weights, integer weights whose total reaches 2^24 and
+    averaged clusters keep the ordered sums."""
+    spec = pkg.synthetic.config_plain(seed=162, n_model=500, n_plane=900, n_box=300)
+    m, s, d = spec.models[0], spec.scene, spec.d_dists[0]
+    scene = pkg.Scene(s, d, 5, context=ctx)
+    cases = [({}, None, 3), ({}, 0.5, 1), ({}, float(1 << 20), 1), ({"use_averaged_clusters": True}, None, 1),
+             ({"cpu_clustering": True}, None, 4)]
+    for kw, w, path in cases:
+        model = pkg.Model(m, d, 0.3, context=ctx, **kw)
+        if w is not None:
+            model.SetModelPointVoteWeights(np.full(len(m), w, np.float32))
+        model.ppf_lookup(scene)
+        assert model.stats["cluster_path"] == path, (kw, w)
