@@ -97,7 +97,7 @@ LookupOut finish_lookup(Context& ctx, Model& m, LookupState& st, const SceneData
   const float min_votecount = m.vote_count_threshold * (float)vr.max_count;
   out.stats.min_votecount = min_votecount;
   out.stats.n_candidates = vr.n_cand;
-  const size_t U = select_votes(ctx, m, s, st, cand_code, cand_count, vr.n_cand, min_votecount);
+  const size_t U = select_votes(ctx, m, s, st, cand_code, cand_count, vr.n_cand, min_votecount, vr.max_count);
   out.stats.n_kept = U;
   if (U == 0) {
     out.status = PPF_ERR_NO_VOTES;

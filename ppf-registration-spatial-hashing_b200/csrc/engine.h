@@ -107,7 +107,7 @@ struct LookupState {
   DevBuf cells3;      // int4 U: integer cell of each pose
   DevBuf qs, tws, adjrun, item_off;  // cell-major clustering tables
   DevBuf item_off32;  // split clustering: (32-target tile, neighbour) items per run
-  DevBuf tmp64, tmp32a, tmp32b, perm;
+  DevBuf tmp64, tmp32a, tmp32b, tmp32c, perm;
   DevBuf tperm;       // clustering target order (cell, rotation bucket)
   DevBuf best;        // float[16] pose + int idx
   uint32_t cluster_path = 0;  // ppf_stats::cluster_path of the last clustering
@@ -171,7 +171,7 @@ void vote_cells_noalloc(Context& ctx, const Model& m, const float* xyz, const fl
 // code asc); returns U.
 size_t select_votes(Context& ctx, const Model& m, const SceneData& s, LookupState& st,
                     const unsigned long long* cand_code, const uint32_t* cand_count, size_t n_cand,
-                    float min_votecount);
+                    float min_votecount, uint32_t max_count);
 // Orders arbitrary (code, count) pairs by code ascending (all-votes dump).
 void sort_by_code(Context& ctx, LookupState& st, size_t n);
 void compute_poses(Context& ctx, const Model& m, const SceneData& s, LookupState& st);

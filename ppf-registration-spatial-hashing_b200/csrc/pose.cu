@@ -43,15 +43,37 @@ __global__ void count_key_kernel(const uint32_t* __restrict__ count, size_t n,
     key[i] = ~__float_as_uint((float)count[i]);
 }
 
-__global__ void gather_kernel(const uint32_t* __restrict__ perm,
-                              const unsigned long long* __restrict__ code_in,
-                              const uint32_t* __restrict__ count_in, size_t n,
-                              unsigned long long* __restrict__ code_out,
-                              uint32_t* __restrict__ count_out) {
+// Descending count as max_count - count.  For counts below 2^24 the float
+// order of the reference's sort and the integer order agree, and the key
+// needs only the bits of max_count.
+__global__ void count_desc_kernel(const uint32_t* __restrict__ count, size_t n, uint32_t max_count,
+                                  uint32_t* __restrict__ key) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    key[i] = max_count - count[i];
+}
+
+// Vote codes s_r << 32 | m_r << 6 | bin packed to s_r << kb | m_r << 6 | bin,
+// kb = 6 + the bits of the largest m_r: the same order in fewer bits.
+template <typename K>
+__global__ void pack_codes_kernel(const unsigned long long* code, size_t n, int kb, K* out) {  // may alias
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
-    uint32_t p = perm[i];
-    code_out[i] = code_in[p];
+    const unsigned long long c = code[i];
+    out[i] = (K)(((c >> 32) << kb) | (uint32_t)c);
+  }
+}
+
+template <typename K>
+__global__ void gather_packed_kernel(const uint32_t* __restrict__ perm, const K* __restrict__ packed,
+                                     const uint32_t* __restrict__ count_in, size_t n, int kb,
+                                     unsigned long long* __restrict__ code_out,
+                                     uint32_t* __restrict__ count_out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t p = perm[i];
+    const unsigned long long k = packed[p];
+    code_out[i] = ((k >> kb) << 32) | (k & ((1ull << kb) - 1));
     count_out[i] = count_in[p];
   }
 }
@@ -594,7 +616,7 @@ T* grow(DevBuf& b, size_t n) {
 
 size_t select_votes(Context& ctx, const Model& m, const SceneData& s, LookupState& st,
                     const unsigned long long* cand_code, const uint32_t* cand_count, size_t n_cand,
-                    float min_votecount) {
+                    float min_votecount, uint32_t max_count) {
   cudaStream_t stream = ctx.stream;
   unsigned long long* fcode = grow<unsigned long long>(st.tmp64, n_cand + 1);
   uint32_t* fcount = grow<uint32_t>(st.tmp32a, n_cand + 1);
@@ -609,22 +631,46 @@ size_t select_votes(Context& ctx, const Model& m, const SceneData& s, LookupStat
   PPF_CUDA(cudaStreamSynchronize(stream));
   st.U = U;
   if (U == 0) return 0;
-  // code ascending (codes are unique), counts carried as values
-  int end_bit = 33;
-  while (end_bit < 64 && ((unsigned long long)s.n >> (end_bit - 32)) != 0) ++end_bit;
+  // code ascending (codes are unique), counts carried as values; codes are
+  // packed to the bits that s_r and m_r need
+  auto bits_for = [](uint64_t x) {
+    int b = 0;
+    while (b < 64 && (x >> b) != 0) ++b;
+    return b;
+  };
+  const int kb = 6 + bits_for(m.t.n > 1 ? m.t.n - 1 : 1);
+  const int code_bits = kb + bits_for(s.n > 1 ? s.n - 1 : 1);
   PPF_CUDA(cudaMemsetAsync(ctx.flags.ptr, 0, 4, stream));
   size_t l0 = ctx.sort64.launches() + ctx.sort32.launches();
-  ctx.sort64.sort(fcode, fcount, false, U, 0, end_bit, stream, ctx.flags.as<uint32_t>());
+  uint32_t* packed32 = nullptr;
+  if (code_bits <= 32) {
+    packed32 = grow<uint32_t>(st.tmp32c, U);
+    pack_codes_kernel<uint32_t><<<grid_for(U, 256), 256, 0, stream>>>(fcode, U, kb, packed32);
+    ctx.sort32.sort(packed32, fcount, false, U, 0, code_bits, stream, ctx.flags.as<uint32_t>());
+  } else {
+    pack_codes_kernel<unsigned long long><<<grid_for(U, 256), 256, 0, stream>>>(fcode, U, kb, fcode);
+    ctx.sort64.sort(fcode, fcount, false, U, 0, code_bits, stream, ctx.flags.as<uint32_t>());
+  }
   // then stable by count descending
   uint32_t* key2 = grow<uint32_t>(st.tmp32b, U);
   uint32_t* perm = grow<uint32_t>(st.perm, U);
-  count_key_kernel<<<grid_for(U, 256), 256, 0, stream>>>(fcount, U, key2);
-  ctx.sort32.sort(key2, perm, true, U, 0, 32, stream, ctx.flags.as<uint32_t>());
-  gather_kernel<<<grid_for(U, 256), 256, 0, stream>>>(perm, fcode, fcount, U,
-                                                       grow<unsigned long long>(st.codes, U),
-                                                       grow<uint32_t>(st.counts, U));
+  if (max_count < (1u << 24)) {
+    count_desc_kernel<<<grid_for(U, 256), 256, 0, stream>>>(fcount, U, max_count, key2);
+    ctx.sort32.sort(key2, perm, true, U, 0, std::max(1, bits_for(max_count)), stream, ctx.flags.as<uint32_t>());
+  } else {
+    count_key_kernel<<<grid_for(U, 256), 256, 0, stream>>>(fcount, U, key2);
+    ctx.sort32.sort(key2, perm, true, U, 0, 32, stream, ctx.flags.as<uint32_t>());
+  }
+  unsigned long long* codes = grow<unsigned long long>(st.codes, U);
+  uint32_t* counts = grow<uint32_t>(st.counts, U);
+  if (packed32)
+    gather_packed_kernel<uint32_t><<<grid_for(U, 256), 256, 0, stream>>>(perm, packed32, fcount, U, kb, codes,
+                                                                         counts);
+  else
+    gather_packed_kernel<unsigned long long><<<grid_for(U, 256), 256, 0, stream>>>(perm, fcode, fcount, U, kb,
+                                                                                   codes, counts);
   PPF_CUDA(cudaGetLastError());
-  ctx.launches += 2 + (ctx.sort64.launches() + ctx.sort32.launches() - l0);
+  ctx.launches += 3 + (ctx.sort64.launches() + ctx.sort32.launches() - l0);
   return U;
 }
 
