@@ -148,6 +148,14 @@ def workload(seed=1001):
     return pkg, spec
 
 
+def workload_name(spec, avg):
+    """The bench workload as named in both arms' JSON lines."""
+    return ("multi-model scene: 4 models (superellipsoid/torus/capsules/spheres-on-slab, "
+            f"{'/'.join(str(len(m)) for m in spec.models)} pts), {len(spec.scene)}-pt scene, "
+            "ref_point_df=5, tau_d=0.03/0.035/0.03/0.05, vote_count_threshold=0.3, GPU clustering, "
+            f"use_averaged_clusters={'on' if avg else 'off'}")
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -198,9 +206,7 @@ def run_reference_arm(args):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * len(spec.models) / cb["value"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "multi-model scene: 4 models (3k-6k pts), 60k-pt scene, ref_point_df=5, "
-                                   "tau_d=0.03/0.035/0.03/0.05, vote_count_threshold=0.3, GPU clustering",
-                       "parallelism": "host threads"},
+            "config": {"workload": workload_name(spec, args.avg), "parallelism": "host threads"},
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference runs this path only on the GPU and cannot at this size (int pair indexing "
@@ -488,10 +494,7 @@ def main():
         "dtype": "f32",
         "data": "synthetic",
         "config": {
-            "workload": "multi-model scene: 4 models (superellipsoid/torus/capsules/spheres-on-slab, "
-                        f"{'/'.join(str(len(m)) for m in spec.models)} pts), {len(spec.scene)}-pt scene, "
-                        "ref_point_df=5, tau_d=0.03/0.035/0.03/0.05, vote_count_threshold=0.3, GPU clustering, "
-                        f"use_averaged_clusters={'on' if args.avg else 'off'}",
+            "workload": workload_name(spec, args.avg),
             "parallelism": f"replicas x{world}",
             "l2": "256 MB L2 flush after every timed step; per-step model tables (~1 GB) exceed L2",
         },
