@@ -58,3 +58,27 @@ def test_missing_library_fails_loudly(pkg, tmp_path):
     capi = import_module("ppf_b200._capi")
     with pytest.raises(RuntimeError, match="missing"):
         capi.load(tmp_path / "nope.so")
+
+
+def test_stats_layout_matches_header(tmp_path):
+    """The ctypes mirror of ppf_stats has the C header's size and field
+    offsets (compiled with gcc)."""
+    import ctypes as C
+    from importlib import import_module
+    from pathlib import Path
+
+    capi = import_module("ppf_b200._capi")
+    S = capi.ppf_stats
+    inc = Path(__file__).resolve().parents[1] / "include"
+    names = [n for n, _ in S._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "ppf_b200.h"\nint main(void) {\n'
+                   '  printf("%zu\\n", sizeof(ppf_stats));\n'
+                   + "".join(f'  printf("%zu\\n", offsetof(ppf_stats, {n}));\n' for n in names)
+                   + "  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    r = subprocess.run(["gcc", "-std=c99", "-I", str(inc), str(src), "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert got[0] == C.sizeof(S)
+    assert got[1:] == [getattr(S, n).offset for n in names]
