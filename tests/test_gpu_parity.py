@@ -28,6 +28,8 @@ CASES = {
     "small": (31, 300, 500, 200, 5, 0.3),
     "medium": (32, 700, 1500, 500, 5, 0.3),
     "df1": (33, 250, 300, 150, 1, 0.4),
+    # 1800 model points: two m_r chunks of 900 rows in the vote accumulator
+    "twochunk": (34, 1800, 1200, 400, 5, 0.3),
 }
 
 
