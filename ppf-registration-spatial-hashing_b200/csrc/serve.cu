@@ -228,7 +228,8 @@ ppf_status server_wait(Server* srv, uint64_t ticket, float* poses, ppf_stats* st
     PPF_REQUIRE(it != srv->tickets.end(), PPF_ERR_INVALID_ARGUMENT, "unknown or already collected ticket");
     r = it->second;
     srv->cv_done.wait(lk, [&] { return r->done; });
-    srv->tickets.erase(it);
+    // by key: another waiter on the same ticket may have erased it meanwhile
+    srv->tickets.erase(ticket);
   }
   if (poses && !r->poses.empty()) std::memcpy(poses, r->poses.data(), r->poses.size() * sizeof(float));
   if (stats && !r->stats.empty()) std::memcpy(stats, r->stats.data(), r->stats.size() * sizeof(ppf_stats));
