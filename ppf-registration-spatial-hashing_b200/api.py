@@ -12,6 +12,7 @@ contiguous CUDA tensors (device, passed by pointer).
 from __future__ import annotations
 
 import ctypes as C
+import threading
 
 import numpy as np
 
@@ -477,6 +478,10 @@ class Server:
         _check(_lib().ppf_server_create(int(device), len(self.models), arr, int(memory_budget), int(workers),
                                         int(max_batch), C.byref(h)))
         self.handle = h
+        # ticket -> number of target models: wait() sizes the pose buffer
+        # that the library fills from it
+        self._targets = {}
+        self._lock = threading.Lock()
 
     def submit(self, cloud, model_ids, ref_point_downsample_factor: int = 1) -> int:
         p, q = _split_cloud(cloud)
@@ -487,12 +492,15 @@ class Server:
         t = C.c_uint64()
         _check(_lib().ppf_server_submit(self.handle, bp.ptr, bq.ptr, bp.n, int(ref_point_downsample_factor),
                                         ids.size, C.c_void_p(ids.ctypes.data), C.byref(t)))
-        self._targets = getattr(self, "_targets", {})
-        self._targets[t.value] = ids.size
+        with self._lock:
+            self._targets[t.value] = ids.size
         return t.value
 
     def wait(self, ticket: int, raise_on_no_votes: bool = True):
-        k = self._targets.pop(ticket, 1)
+        with self._lock:
+            k = self._targets.pop(int(ticket), None)
+        if k is None:  # the library's own answer for a ticket it does not hold
+            raise PPFError(1, f"unknown or already collected ticket {ticket}")
         poses = np.zeros((k, 16), np.float32)
         stats = (_capi.ppf_stats * k)()
         lat = C.c_double()

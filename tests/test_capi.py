@@ -82,3 +82,15 @@ def test_stats_layout_matches_header(tmp_path):
     got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     assert got[0] == C.sizeof(S)
     assert got[1:] == [getattr(S, n).offset for n in names]
+
+
+def test_server_wait_needs_a_known_ticket(pkg):
+    """Server.wait sizes the pose buffer the library fills from the ticket's
+    target count; a ticket it did not issue, or one already collected, is
+    refused before the library is called."""
+    import threading
+
+    srv = object.__new__(pkg.Server)
+    srv._targets, srv._lock, srv.handle = {}, threading.Lock(), None
+    with pytest.raises(pkg.PPFError, match="unknown or already collected"):
+        srv.wait(5)
