@@ -68,7 +68,9 @@ int ppf_abi_version(void);
 /* Device selection as ppf_registration's devUse: device min(count-1, device)
  * (src/cuda/ppf.cu:37-49).  The context owns a CUDA stream and a workspace;
  * it never resets the device (the reference calls cudaDeviceReset at the end
- * of ppf_registration, src/cuda/ppf.cu:103). */
+ * of ppf_registration, src/cuda/ppf.cu:103).  Models and scenes keep using
+ * the context that made them, up to and including their destroy call:
+ * destroy them (and any server over them) before the context. */
 ppf_status ppf_context_create(int device, ppf_context_t* out);
 ppf_status ppf_context_destroy(ppf_context_t ctx);
 ppf_status ppf_context_synchronize(ppf_context_t ctx);
