@@ -78,6 +78,8 @@ ppf_status ppf_context_synchronize(ppf_context_t ctx);
 void* ppf_context_stream(ppf_context_t ctx);
 /* Kernels this context has launched so far (running total). */
 uint64_t ppf_context_kernel_launches(ppf_context_t ctx);
+/* The CUDA device index the context runs on (-1 for a null context). */
+int ppf_context_device(ppf_context_t ctx);
 
 /* Model::Model(cloud, d_dist, vote_count_threshold, cpu_clustering,
  * use_l1_norm, use_averaged_clusters) (include/model.h:17-19,
@@ -93,6 +95,11 @@ ppf_status ppf_model_set_point_vote_weights(ppf_model_t m, const float* w, uint6
 ppf_status ppf_model_destroy(ppf_model_t m);
 uint64_t ppf_model_num_points(ppf_model_t m);
 uint64_t ppf_model_num_keys(ppf_model_t m); /* unique feature keys K */
+/* Chunks of model reference points the vote pass splits the model into: one
+ * chunk's (m_r, alpha) counters fill one block's shared memory, so a scene
+ * reference point is one work item per chunk.  No counterpart in the
+ * reference, which keeps every vote in global memory. */
+uint64_t ppf_model_num_chunks(ppf_model_t m);
 
 /* Scene::Scene(cloud, d_dist, ref_point_downsample_factor)
  * (include/scene.h:15-16, src/cuda/scene.cu:24-55).  Scene pair features are
@@ -278,10 +285,9 @@ ppf_status ppf_model_pair_vote_counts(ppf_model_t m, ppf_scene_t s, uint64_t* co
  * Scratch: counters, the work items that did not fit and the scene packed to
  * float4 live in one static device array of 3 MiB + 256 B in the library,
  * which every GPU that loads the library holds until the process exits.
- * Limits: n_scene <= 65536 points and ceil(n_scene / ref_point_df) x model
- * chunks <= 262144 work items (a model of n points has ceil(n / 1659) chunks
- * on a B200); larger inputs return PPF_ERR_INVALID_ARGUMENT before any GPU
- * work.  The call zeroes the scratch's 256-byte counter header on the
+ * Limits: n_scene <= 65536 points and ceil(n_scene / ref_point_df) x
+ * ppf_model_num_chunks(m) <= 262144 work items; larger inputs return
+ * PPF_ERR_INVALID_ARGUMENT before any GPU work.  The call zeroes the scratch's 256-byte counter header on the
  * context's stream before its kernels; nothing the caller passes needs to
  * start at zero.  Output too small: PPF_ERR_OUT_OF_MEMORY, *n_out = the cells
  * this call needed (the cells of the work items that fit were written).
@@ -290,8 +296,10 @@ ppf_status ppf_model_pair_vote_counts(ppf_model_t m, ppf_scene_t s, uint64_t* co
  * (cudaGetSymbolAddress) with that device current; make that first call
  * before any stream capture.  All calls on one device share the array:
  * calls that overlap in time (other threads, contexts or streams on the same
- * device) race on it, so the caller serialises them.  Returns after the
- * context's stream has finished the pass. */
+ * device) race on it, so the caller serialises them.  Each call sets the
+ * vote kernel's shared-memory attribute, reads its counters back into host
+ * memory and waits for the context's stream (cudaStreamSynchronize) before
+ * it returns. */
 ppf_status ppf_model_vote_cells_noalloc(ppf_model_t m, const float* scene_xyz,
                                         const float* scene_nxyz, uint64_t n_scene,
                                         uint32_t ref_point_df, float vote_floor, uint64_t* codes,

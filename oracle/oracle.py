@@ -71,6 +71,7 @@ class orc_params(C.Structure):
         ("sr_begin", C.c_int64),
         ("sr_end", C.c_int64),
         ("sr_step", C.c_int64),
+        ("votes_only", C.c_int),
     ]
 
 
@@ -176,12 +177,14 @@ class Oracle:
         return out
 
     def register(self, model, scene, d_dist, ref_df=1, thr=0.4, cpu_clustering=False, use_l1_norm=False,
-                 use_averaged_clusters=False, weights=None, n_threads=0, sr_range=None, sr_step=0):
+                 use_averaged_clusters=False, weights=None, n_threads=0, sr_range=None, sr_step=0,
+                 votes_only=False):
         mp, mn = _f32(model[0]), _f32(model[1])
         sp, sn = _f32(scene[0]), _f32(scene[1])
         prm = orc_params(float(d_dist), int(ref_df), float(thr), int(cpu_clustering), int(use_l1_norm),
                          int(use_averaged_clusters), int(n_threads),
-                         sr_range[0] if sr_range else 0, sr_range[1] if sr_range else -1, int(sr_step))
+                         sr_range[0] if sr_range else 0, sr_range[1] if sr_range else -1, int(sr_step),
+                         int(bool(votes_only)))
         w = _f32(weights) if weights is not None else None
         r = self.L.orc_register(_p(mp), _p(mn), mp.shape[0], _p(sp), _p(sn), sp.shape[0],
                                 _p(w) if w is not None else None, C.byref(prm))
@@ -320,6 +323,12 @@ class RefGPU:
             C.POINTER(rh_result), _u64p, _u32p, C.c_longlong, _u64p, _u32p, _fp, _fp, _fp, _fp,
             C.c_longlong, _u64p,
         ]
+        L.rh_unique_votes.restype = C.c_int
+        L.rh_unique_votes.argtypes = [_fp, _fp, C.c_int, _fp, _fp, C.c_int, C.c_float, C.c_uint,
+                                      C.POINTER(rh_result), _u64p, _u32p, C.c_longlong]
+        L.rh_post.restype = C.c_int
+        L.rh_post.argtypes = [_fp, _fp, C.c_int, _fp, _fp, C.c_int, C.c_float, C.c_int, C.c_int, _fp, _u64p,
+                              _u32p, C.c_longlong, C.POINTER(rh_result), _fp, _fp, _fp, _fp]
         self.L = L
 
     def _err(self, rc, what):
@@ -396,6 +405,46 @@ class RefGPU:
         if pc is not None:
             out["pair_counts"] = pc.reshape(ns, ns)
         return out
+
+    def unique_votes(self, model, scene, d_dist, ref_df=1, cap=1 << 24):
+        """Every nonzero (s_r, m_r, alpha) vote cell in code order with its
+        count (the reference's unique votes before the threshold)."""
+        mp, mn = _f32(model[0]), _f32(model[1])
+        sp, sn = _f32(scene[0]), _f32(scene[1])
+        res = rh_result()
+        codes = np.zeros(cap, np.uint64)
+        counts = np.zeros(cap, np.uint32)
+        rc = self.L.rh_unique_votes(_p(mp), _p(mn), mp.shape[0], _p(sp), _p(sn), sp.shape[0], float(d_dist),
+                                    int(ref_df), C.byref(res), _p(codes, _u64p), _p(counts, _u32p), cap)
+        self._err(rc, "rh_unique_votes")
+        nu = int(res.n_unique)
+        if nu > cap:
+            return self.unique_votes(model, scene, d_dist, ref_df, cap=nu)
+        return {"codes": codes[:nu], "counts": counts[:nu], "n_votes": int(res.n_votes),
+                "elapsed_ms": float(res.elapsed_ms)}
+
+    def post(self, model, scene, d_dist, codes, counts, use_l1_norm=False, use_averaged_clusters=False,
+             weights=None):
+        """Poses, weighted counts, clustering and the best pose of kept votes
+        given in the reference's order (count descending, code ascending)."""
+        mp, mn = _f32(model[0]), _f32(model[1])
+        sp, sn = _f32(scene[0]), _f32(scene[1])
+        c = np.ascontiguousarray(np.asarray(codes, np.uint64))
+        k = np.ascontiguousarray(np.asarray(counts, np.uint32))
+        U = c.size
+        res = rh_result()
+        T = np.zeros(U * 16, np.float32)
+        t = np.zeros(U * 3, np.float32)
+        q = np.zeros(U * 4, np.float32)
+        s = np.zeros(U, np.float32)
+        w = _f32(weights) if weights is not None else None
+        rc = self.L.rh_post(_p(mp), _p(mn), mp.shape[0], _p(sp), _p(sn), sp.shape[0], float(d_dist),
+                            int(use_l1_norm), int(use_averaged_clusters), _p(w) if w is not None else None,
+                            _p(c, _u64p), _p(k, _u32p), U, C.byref(res), _p(T), _p(t), _p(q), _p(s))
+        self._err(rc, "rh_post")
+        return {"max_idx": int(res.max_idx), "pose": np.array(res.pose[:], np.float32).reshape(4, 4),
+                "transforms": T.reshape(-1, 16), "trans": t.reshape(-1, 3), "quats": q.reshape(-1, 4),
+                "scores": s, "elapsed_ms": float(res.elapsed_ms)}
 
 
 def available(kind: str) -> bool:

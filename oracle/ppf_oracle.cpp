@@ -590,6 +590,10 @@ orc_result* orc_register(const float* m_pts, const float* m_nrm, int64_t n_m, co
                          const float* s_nrm, int64_t n_s, const float* model_weights,
                          const orc_params* prm) {
   orc_result* R = (orc_result*)calloc(1, sizeof(orc_result));
+  if (n_m > 65536) {  // m_r is kept in 16 bits per model pair below
+    R->status = -2;
+    return R;
+  }
   typedef std::chrono::steady_clock Clk;
   const Clk::time_point t0 = Clk::now();
   const float d = prm->d_dist;
@@ -611,6 +615,26 @@ orc_result* orc_register(const float* m_pts, const float* m_nrm, int64_t n_m, co
     M4 T;
     frame(ld3(m_pts + 3 * r), ld3(m_nrm + 3 * r), T);
     memcpy(&mframe[16 * r], T, sizeof(T));
+  }
+  // u = m_i in the frame of m_r for every entry of the hash array, in hash
+  // array order (only its y and z enter alpha, kernel.cu:338-342), and the
+  // entry's m_r: the same bits trans_model_scene recomputes per vote
+  // (kernel.cu:329-336), computed once per model pair.
+  const size_t n_pairs = H.map.size();
+  std::vector<float> u_yz(2 * n_pairs);
+  std::vector<uint16_t> u_mr(n_pairs);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static)
+#endif
+  for (int64_t j = 0; j < (int64_t)n_pairs; ++j) {
+    const uint32_t pair = H.map[j];
+    const uint32_t mr = pair / (uint32_t)n_m, mi = pair - mr * (uint32_t)n_m;
+    M4 Tm;
+    memcpy(Tm, &mframe[16 * mr], sizeof(Tm));
+    const F3 u = frame_apply(Tm, ld3(m_pts + 3 * mi));
+    u_yz[2 * j] = u.y;
+    u_yz[2 * j + 1] = u.z;
+    u_mr[j] = (uint16_t)mr;
   }
   const Clk::time_point t1 = Clk::now();
   R->t_build = std::chrono::duration<double>(t1 - t0).count();
@@ -653,14 +677,10 @@ orc_result* orc_register(const float* m_pts, const float* m_nrm, int64_t n_m, co
           F3 v = frame_apply(Ts, ld3(s_pts + 3 * si));
           uint32_t first = H.first[run], cnt = H.counts[run];
           nv += cnt;
-          for (uint32_t e = 0; e < cnt; ++e) {
-            uint32_t pair = H.map[first + e];
-            uint32_t mr = pair / (uint32_t)n_m, mi = pair - mr * (uint32_t)n_m;
-            M4 Tm;
-            memcpy(Tm, &mframe[16 * mr], sizeof(Tm));
-            F3 u = frame_apply(Tm, ld3(m_pts + 3 * mi));
+          for (uint32_t e = first; e < first + cnt; ++e) {
+            const F3 u{0.f, u_yz[2 * (size_t)e], u_yz[2 * (size_t)e + 1]};
             uint32_t bin = alpha_bin(u, v);
-            acc[(size_t)mr * nb + bin]++;
+            acc[(size_t)u_mr[e] * nb + bin]++;
           }
         }
         uint32_t lmax = 0;
@@ -720,6 +740,7 @@ orc_result* orc_register(const float* m_pts, const float* m_nrm, int64_t n_m, co
     R->codes[i] = kept[i].code;
     R->counts[i] = kept[i].count;
   }
+  if (prm->votes_only) return R;
   // Every per-vote kernel returns early for count <= 1 (kernel.cu:609 etc.),
   // so a single kept vote leaves all derived arrays at zero.
   const bool run_kernels = U > 1;

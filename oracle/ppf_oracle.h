@@ -103,6 +103,9 @@ typedef struct orc_params {
   int64_t sr_begin, sr_end;
   /* step between processed reference points; 0 means ref_point_df */
   int64_t sr_step;
+  /* nonzero: stop after the threshold (codes and counts only; no poses or
+   * clustering).  With vote_count_threshold 0 this gives every nonzero cell. */
+  int votes_only;
 } orc_params;
 
 /* Model::Model + Model::ppf_lookup + pose extraction for one (scene, model). */

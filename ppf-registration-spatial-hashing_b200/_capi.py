@@ -58,6 +58,7 @@ SIGNATURES = {
     "ppf_context_synchronize": (C.c_int, [_vp]),
     "ppf_context_stream": (_vp, [_vp]),
     "ppf_context_kernel_launches": (C.c_uint64, [_vp]),
+    "ppf_context_device": (C.c_int, [_vp]),
     "ppf_model_create": (
         C.c_int,
         [_vp, _vp, _vp, C.c_uint64, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int, C.POINTER(_vp)],
@@ -66,6 +67,7 @@ SIGNATURES = {
     "ppf_model_destroy": (C.c_int, [_vp]),
     "ppf_model_num_points": (C.c_uint64, [_vp]),
     "ppf_model_num_keys": (C.c_uint64, [_vp]),
+    "ppf_model_num_chunks": (C.c_uint64, [_vp]),
     "ppf_scene_create": (C.c_int, [_vp, _vp, _vp, C.c_uint64, C.c_float, C.c_uint32, C.POINTER(_vp)]),
     "ppf_scene_destroy": (C.c_int, [_vp]),
     "ppf_model_lookup": (C.c_int, [_vp, _vp, _vp, C.POINTER(ppf_stats)]),

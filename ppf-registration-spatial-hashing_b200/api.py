@@ -79,6 +79,11 @@ class Context:
     def stream(self) -> int:
         return int(_lib().ppf_context_stream(self.handle) or 0)
 
+    @property
+    def device(self) -> int:
+        """The CUDA device index the context runs on."""
+        return int(_lib().ppf_context_device(self.handle))
+
     def close(self):
         if getattr(self, "handle", None):
             _lib().ppf_context_destroy(self.handle)
@@ -182,6 +187,11 @@ class Model:
         return self.pose
 
     @property
+    def num_chunks(self) -> int:
+        """Chunks of model reference points per scene reference point in the vote pass."""
+        return int(_lib().ppf_model_num_chunks(self.handle))
+
+    @property
     def max_idx(self) -> int:
         return int(self.stats["max_idx"]) if self.stats else 0
 
@@ -274,6 +284,9 @@ class Model:
                             ("counts_out", counts_out, ("torch.int32", "torch.uint32"))):
             if not (hasattr(t, "is_cuda") and t.is_cuda and t.is_contiguous() and repr(t.dtype) in dt):
                 raise ValueError(f"{name}: expected a contiguous CUDA tensor of {' or '.join(dt)}")
+            if t.device.index != self.ctx.device:
+                raise ValueError(f"{name}: tensor on cuda:{t.device.index}, model's context on "
+                                 f"cuda:{self.ctx.device}")
         if scene_xyz.shape != scene_nxyz.shape or scene_xyz.dim() != 2 or scene_xyz.shape[1] != 3:
             raise ValueError("scene_xyz / scene_nxyz: expected two (n, 3) tensors")
         if codes_out.numel() != counts_out.numel():

@@ -272,6 +272,7 @@ ppf_status ppf_context_synchronize(ppf_context_t ctx) {
 
 void* ppf_context_stream(ppf_context_t ctx) { return ctx ? (void*)ctx->c.stream : nullptr; }
 uint64_t ppf_context_kernel_launches(ppf_context_t ctx) { return ctx ? ctx->c.launches : 0; }
+int ppf_context_device(ppf_context_t ctx) { return ctx ? ctx->c.device : -1; }
 
 ppf_status ppf_model_create(ppf_context_t ctx, const float* xyz, const float* nxyz, uint64_t n,
                             float d_dist, float vote_count_threshold, int cpu_clustering,
@@ -322,6 +323,7 @@ ppf_status ppf_model_destroy(ppf_model_t m) {
 
 uint64_t ppf_model_num_points(ppf_model_t m) { return m ? m->m.t.n : 0; }
 uint64_t ppf_model_num_keys(ppf_model_t m) { return m ? m->m.t.K : 0; }
+uint64_t ppf_model_num_chunks(ppf_model_t m) { return m ? m->m.t.n_chunks : 0; }
 
 ppf_status ppf_scene_create(ppf_context_t ctx, const float* xyz, const float* nxyz, uint64_t n,
                             float d_dist, uint32_t ref_point_df, ppf_scene_t* out) {
@@ -405,7 +407,7 @@ ppf_status ppf_lookup_batch(ppf_context_t ctx, uint64_t n, const ppf_model_t* mo
 namespace {
 // n x 3 floats on the device: the caller's pointer, or a copy of host memory
 const float* device_xyz(Context& c, const float* p, size_t n, DevBuf& tmp) {
-  if (is_device_pointer(p)) return p;
+  if (is_device_pointer(p, c.device)) return p;
   tmp.reserve(std::max<size_t>(n, 1) * 12);
   if (n) PPF_CUDA(cudaMemcpyAsync(tmp.ptr, p, n * 12, cudaMemcpyHostToDevice, c.stream));
   return tmp.as<float>();
@@ -459,12 +461,12 @@ ppf_status ppf_cluster_poses(ppf_context_t ctx, const float* transforms, const u
     DevBuf tT, tV;
     const float* T = transforms;
     const uint32_t* V = votes;
-    if (n && !is_device_pointer(transforms)) {
+    if (n && !is_device_pointer(transforms, ctx->c.device)) {
       tT.reserve(n * 64);
       PPF_CUDA(cudaMemcpyAsync(tT.ptr, transforms, n * 64, cudaMemcpyHostToDevice, ctx->c.stream));
       T = tT.as<float>();
     }
-    if (n && !is_device_pointer(votes)) {
+    if (n && !is_device_pointer(votes, ctx->c.device)) {
       tV.reserve(n * 4);
       PPF_CUDA(cudaMemcpyAsync(tV.ptr, votes, n * 4, cudaMemcpyHostToDevice, ctx->c.stream));
       V = tV.as<uint32_t>();
@@ -700,7 +702,7 @@ ppf_status ppf_pair_keys(ppf_context_t ctx, const float* xyz, const float* nxyz,
     upload_points(c, xyz, n, p);
     upload_points(c, nxyz, n, q);
     uint32_t* dst = keys;
-    if (!is_device_pointer(keys)) {
+    if (!is_device_pointer(keys, c.device)) {
       k.reserve(n * n * 4);
       dst = k.as<uint32_t>();
     }
@@ -756,7 +758,7 @@ ppf_status ppf_model_pair_vote_counts(ppf_model_t m, ppf_scene_t s, uint64_t* co
     const size_t nn = (size_t)s->s.n * s->s.n;
     DevBuf tmp;
     uint64_t* dst = counts;
-    if (!is_device_pointer(counts)) {
+    if (!is_device_pointer(counts, c.device)) {
       tmp.reserve(nn * 8);
       dst = tmp.as<uint64_t>();
     }

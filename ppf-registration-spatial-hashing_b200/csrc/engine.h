@@ -131,7 +131,11 @@ void pair_keys_device(Context& ctx, const float4* pts, const float4* nrm, uint32
                       uint32_t ref_df, float d_dist, uint32_t* keys);
 // upload n x 3 floats (host or device) into a float4 device array
 void upload_points(Context& ctx, const float* xyz, size_t n, DevBuf& dst);
-bool is_device_pointer(const void* p);
+// Device memory of `device` or managed memory: true; host memory: false.
+// Device memory of another GPU raises PPF_ERR_INVALID_ARGUMENT.
+bool is_device_pointer(const void* p, int device);
+// Device or managed memory of any GPU.
+bool is_any_device_pointer(const void* p);
 
 // ---- voting (vote.cu)
 struct VoteResult {

@@ -206,7 +206,7 @@ __global__ void fill_f32(float* p, size_t n, float v) {
 
 }  // namespace
 
-bool is_device_pointer(const void* p) {
+bool is_any_device_pointer(const void* p) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
@@ -215,12 +215,28 @@ bool is_device_pointer(const void* p) {
   return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+bool is_device_pointer(const void* p, int device) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (a.type == cudaMemoryTypeManaged) return true;
+  if (a.type != cudaMemoryTypeDevice) return false;
+  // A kernel of this context would read another GPU's memory as a peer
+  // without peer access enabled: refused before any launch.
+  PPF_REQUIRE(a.device == device, PPF_ERR_INVALID_ARGUMENT,
+              "device pointer on GPU " + std::to_string(a.device) + " passed to a context on GPU " +
+                  std::to_string(device));
+  return true;
+}
+
 void upload_points(Context& ctx, const float* xyz, size_t n, DevBuf& dst) {
   dst.reserve(n * sizeof(float4));
   if (n == 0) return;
   DevBuf tmp;
   const float* src = xyz;
-  if (!is_device_pointer(xyz)) {
+  if (!is_device_pointer(xyz, ctx.device)) {
     tmp.reserve(n * 3 * sizeof(float));
     PPF_CUDA(cudaMemcpyAsync(tmp.ptr, xyz, n * 3 * sizeof(float), cudaMemcpyHostToDevice,
                              ctx.stream));

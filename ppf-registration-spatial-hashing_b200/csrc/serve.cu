@@ -195,7 +195,7 @@ uint64_t server_submit(Server* srv, const float* xyz, const float* nxyz, uint64_
                        const uint32_t* model_ids, uint64_t n_ids) {
   PPF_REQUIRE(xyz && nxyz && n >= 1 && n < (1ull << 31), PPF_ERR_INVALID_ARGUMENT, "bad scene cloud");
   PPF_REQUIRE(model_ids && n_ids >= 1, PPF_ERR_INVALID_ARGUMENT, "no target models");
-  PPF_REQUIRE(!is_device_pointer(xyz) && !is_device_pointer(nxyz), PPF_ERR_INVALID_ARGUMENT,
+  PPF_REQUIRE(!is_any_device_pointer(xyz) && !is_any_device_pointer(nxyz), PPF_ERR_INVALID_ARGUMENT,
               "submitted clouds must be host memory");
   auto r = std::make_shared<Request>();
   r->xyz.assign(xyz, xyz + 3 * n);

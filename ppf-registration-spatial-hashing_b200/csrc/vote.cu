@@ -912,9 +912,10 @@ void vote_cells_noalloc(Context& ctx, const Model& m, const float* xyz, const fl
               "scene of " + std::to_string(n) + " points exceeds the allocation-free limit of " +
                   std::to_string(kNoAllocMaxScenePoints));
   if (n < 2) return;
-  PPF_REQUIRE(xyz && nxyz && is_device_pointer(xyz) && is_device_pointer(nxyz),
+  PPF_REQUIRE(xyz && nxyz && is_device_pointer(xyz, ctx.device) && is_device_pointer(nxyz, ctx.device),
               PPF_ERR_INVALID_ARGUMENT, "scene points and normals must be device memory");
-  PPF_REQUIRE(capacity == 0 || (codes && counts && is_device_pointer(codes) && is_device_pointer(counts)),
+  PPF_REQUIRE(capacity == 0 || (codes && counts && is_device_pointer(codes, ctx.device) &&
+                                   is_device_pointer(counts, ctx.device)),
               PPF_ERR_INVALID_ARGUMENT, "vote cell outputs must be device memory");
   PPF_REQUIRE(capacity <= 0xffffffffull, PPF_ERR_INVALID_ARGUMENT, "capacity beyond 2^32 - 1 cells");
   ref_df = ref_df ? ref_df : 1;

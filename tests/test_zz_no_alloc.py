@@ -126,3 +126,44 @@ def test_sizes_beyond_the_limit_are_rejected(pkg, small):
         model.handle, C.c_void_p(host.ctypes.data), C.c_void_p(host.ctypes.data), 100, 1, 0.0,
         C.c_void_p(codes.data_ptr()), C.c_void_p(counts.data_ptr()), 16, C.byref(n), None)
     assert pkg._capi.STATUS_NAMES[st] == "PPF_ERR_INVALID_ARGUMENT"
+
+
+def test_work_items_beyond_the_limit_are_rejected(pkg, ctx):
+    """A scene within the point limit whose reference points times the model's
+    chunks exceed the 262144 work items the static scratch holds is refused
+    before any GPU work."""
+    import torch
+
+    spec = pkg.synthetic.config_plain(seed=73, n_model=9000, n_plane=10, n_box=10)
+    model = pkg.Model(spec.models[0], spec.d_dists[0], 0.3, context=ctx)
+    chunks = model.num_chunks
+    n_scene = 60000
+    assert n_scene <= 65536 and n_scene * chunks > 262144, chunks
+    xyz = torch.zeros((n_scene, 3), dtype=torch.float32, device="cuda")
+    codes, counts = _outputs(16)
+    launches = ctx.kernel_launches
+    with pytest.raises(pkg.PPFError) as e:
+        model.vote_cells_noalloc(xyz, xyz, 1, 0.0, codes, counts)
+    assert pkg._capi.STATUS_NAMES[e.value.status] == "PPF_ERR_INVALID_ARGUMENT"
+    assert "work items" in str(e.value)
+    assert ctx.kernel_launches == launches
+
+
+def test_tensors_on_another_device_are_refused(small):
+    """The Python wrapper compares each tensor's device with the model's
+    context before the call (a stand-in context on another device index
+    makes the mismatch with one GPU)."""
+    spec, model, _ = small
+    xyz, nxyz = _scene_dev(spec.scene)
+    codes, counts = _outputs(16)
+
+    class OtherDevice:
+        device = xyz.device.index + 1
+
+    real = model.ctx
+    model.ctx = OtherDevice()
+    try:
+        with pytest.raises(ValueError, match="context on cuda:"):
+            model.vote_cells_noalloc(xyz, nxyz, spec.ref_point_df, 0.0, codes, counts)
+    finally:
+        model.ctx = real
