@@ -225,6 +225,13 @@ void init_context(Context& c, int device) {
   if (const char* e = std::getenv("PPF_B200_CHECKS")) c.checks = e[0] == '1';
   if (const char* e = std::getenv("PPF_B200_HOST_GREEDY")) c.host_greedy = e[0] == '1';
   if (const char* e = std::getenv("PPF_B200_CLUSTER_SPLIT")) c.cluster_split = e[0] != '0';
+  if (const char* e = std::getenv("PPF_B200_ENTRY_ORDER")) c.entry_spread = std::strcmp(e, "hash") != 0;
+  // test hooks: the n-th device allocation from now fails; the next 32-bit
+  // radix sort on this context has one tile withhold its look-back status,
+  // so that the tiles waiting on it give up after a short bounded spin
+  if (const char* e = std::getenv("PPF_B200_TEST_FAIL_ALLOC")) alloc_failure_countdown() = std::atoll(e);
+  if (const char* e = std::getenv("PPF_B200_TEST_SORT_STALL"))
+    if (e[0] == '1') c.sort32.arm_stall();
   // test hook: a small initial candidate buffer exercises its growth path
   if (const char* e = std::getenv("PPF_B200_CANDIDATE_CAP")) {
     long long v = std::atoll(e);

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <stdexcept>
 #include <string>
 
@@ -48,6 +49,15 @@ struct StreamScope {
   ~StreamScope() { alloc_stream() = prev; }
 };
 
+// Failure injection for tests: when positive, the device allocation that
+// brings it to zero fails with PPF_ERR_OUT_OF_MEMORY as a failed cudaMalloc
+// would.  Armed per process from PPF_B200_TEST_FAIL_ALLOC=<n> when a context
+// is created; zero (off) otherwise.
+inline std::atomic<long long>& alloc_failure_countdown() {
+  static std::atomic<long long> n{0};
+  return n;
+}
+
 // Owning device allocation, grown on demand, never shrunk implicitly.
 struct DevBuf {
   void* ptr = nullptr;
@@ -84,6 +94,9 @@ struct DevBuf {
   }
   void reserve(size_t b) {
     if (b <= bytes) return;
+    if (alloc_failure_countdown().load(std::memory_order_relaxed) > 0 &&
+        alloc_failure_countdown().fetch_sub(1) == 1)
+      throw Error(PPF_ERR_OOM, "device allocation of " + std::to_string(b) + " bytes failed (injected)");
     release();
     size_t want = b < 256 ? 256 : b;
     stream = alloc_stream();

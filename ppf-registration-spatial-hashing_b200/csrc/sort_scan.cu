@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(kThreads) rs_onesweep(
     const K* __restrict__ kin, const uint32_t* __restrict__ vin, bool vin_iota,
     K* __restrict__ kout, uint32_t* __restrict__ vout, size_t n, int shift,
     const uint32_t* __restrict__ pass_hist, unsigned long long* status, uint32_t* tile_counter,
-    uint32_t* flags) {
+    uint32_t* flags, uint32_t stall_tile, int spin_limit) {
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_whist[kWarps][kRadix];
   __shared__ uint32_t s_tile_start[kRadix];
@@ -136,17 +136,18 @@ __global__ void __launch_bounds__(kThreads) rs_onesweep(
   // Decoupled look-back for this digit.
   unsigned long long* my = status + (size_t)tile * kRadix + tid;
   uint32_t excl = 0;
+  const bool publish = tile != stall_tile;  // the test hook's silent tile
   if (tile == 0) {
     store_status(my, kInc | (unsigned long long)tile_cnt);
   } else {
-    store_status(my, kAgg | (unsigned long long)tile_cnt);
+    if (publish) store_status(my, kAgg | (unsigned long long)tile_cnt);
     long long t = (long long)tile - 1;
     while (t >= 0) {
       const unsigned long long* p = status + (size_t)t * kRadix + tid;
       unsigned long long v = load_status(p);
       int spins = 0;
       while ((v >> 32) == 0) {
-        if (++spins > kSpinLimit) {
+        if (++spins > spin_limit) {
           atomicOr(flags, (uint32_t)kFlagSpinTimeout);
           v = kInc;
           break;
@@ -158,7 +159,7 @@ __global__ void __launch_bounds__(kThreads) rs_onesweep(
       if ((v >> 32) == 2) break;
       --t;
     }
-    store_status(my, kInc | (unsigned long long)(excl + tile_cnt));
+    if (publish) store_status(my, kInc | (unsigned long long)(excl + tile_cnt));
   }
   s_global[tid] = pass_base + excl;
   __syncthreads();
@@ -285,12 +286,17 @@ void RadixSorter<K>::sort(K* keys, uint32_t* vals, bool vals_iota, size_t n, int
   K* kout = kalt_.as<K>();
   uint32_t* vout = valt_.as<uint32_t>();
   bool iota = vals_iota;
+  // the test hook (arm_stall) applies to the first pass of a sort with a tile 1
+  const bool stall = stall_ && tiles > 1;
+  if (stall) stall_ = false;
   for (int p = 0; p < passes; ++p) {
     PPF_CUDA(cudaMemsetAsync(status_.ptr, 0, tiles * kRadix * sizeof(unsigned long long), st));
     PPF_CUDA(cudaMemsetAsync(counters_.ptr, 0, sizeof(uint32_t), st));
+    const bool stall_here = stall && p == 0;
     rs_onesweep<K><<<(unsigned)tiles, kThreads, 0, st>>>(
         kin, vin, iota, kout, vout, n, begin_bit + 8 * p, hist_.as<uint32_t>() + p * kRadix,
-        status_.as<unsigned long long>(), counters_.as<uint32_t>(), d_flags);
+        status_.as<unsigned long long>(), counters_.as<uint32_t>(), d_flags, stall_here ? 1u : 0xffffffffu,
+        stall_here ? 4096 : kSpinLimit);
     PPF_CUDA(cudaGetLastError());
     launches_ += 1;
     iota = false;
@@ -300,6 +306,16 @@ void RadixSorter<K>::sort(K* keys, uint32_t* vals, bool vals_iota, size_t n, int
   if (kin != keys) {
     PPF_CUDA(cudaMemcpyAsync(keys, kin, n * sizeof(K), cudaMemcpyDeviceToDevice, st));
     PPF_CUDA(cudaMemcpyAsync(vals, vin, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+  }
+  // A look-back that gave up leaves the order undefined: stop here.
+  uint32_t f = 0;
+  PPF_CUDA(cudaMemcpyAsync(&f, d_flags, sizeof(f), cudaMemcpyDeviceToHost, st));
+  PPF_CUDA(cudaStreamSynchronize(st));
+  if (f & kFlagSpinTimeout) {
+    const uint32_t clear = f & ~(uint32_t)kFlagSpinTimeout;
+    PPF_CUDA(cudaMemcpyAsync(d_flags, &clear, sizeof(clear), cudaMemcpyHostToDevice, st));
+    PPF_CUDA(cudaStreamSynchronize(st));
+    throw Error(PPF_ERR_TIMEOUT, "radix sort look-back timed out (" + std::to_string(n) + " keys)");
   }
 }
 
@@ -311,21 +327,48 @@ void exclusive_scan_small(uint32_t* v, size_t n, uint32_t* total_dev, cudaStream
   PPF_CUDA(cudaGetLastError());
 }
 
-size_t build_runs(const uint32_t* sorted_keys, size_t n, uint32_t* uniq, uint32_t* first,
-                  uint32_t* count, DevBuf& scratch, cudaStream_t st, size_t* launches) {
-  if (n == 0) return 0;
+namespace {
+// Run heads per tile, scanned: scratch[t] = runs before tile t,
+// scratch[tiles] = K.  Returns K (one stream synchronisation).
+size_t count_runs(const uint32_t* sorted_keys, size_t n, DevBuf& scratch, cudaStream_t st) {
   const size_t tiles = (n + kRunTile - 1) / kRunTile;
   scratch.reserve((tiles + 1) * sizeof(uint32_t));
   uint32_t* th = scratch.as<uint32_t>();
   runs_count<<<(unsigned)tiles, kRunThreads, 0, st>>>(sorted_keys, n, th);
   runs_scan_tiles<<<1, kRunThreads, 0, st>>>(th, tiles, th + tiles);
-  runs_emit<<<(unsigned)tiles, kRunThreads, 0, st>>>(sorted_keys, n, th, uniq, first);
   PPF_CUDA(cudaGetLastError());
   uint32_t K = 0;
   PPF_CUDA(cudaMemcpyAsync(&K, th + tiles, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   PPF_CUDA(cudaStreamSynchronize(st));
+  return K;
+}
+
+void emit_runs(const uint32_t* sorted_keys, size_t n, size_t K, uint32_t* uniq, uint32_t* first, uint32_t* count,
+               DevBuf& scratch, cudaStream_t st) {
+  const size_t tiles = (n + kRunTile - 1) / kRunTile;
+  runs_emit<<<(unsigned)tiles, kRunThreads, 0, st>>>(sorted_keys, n, scratch.as<uint32_t>(), uniq, first);
   runs_lengths<<<grid_for(K, 256), 256, 0, st>>>(first, K, n, count);
   PPF_CUDA(cudaGetLastError());
+}
+}  // namespace
+
+size_t build_runs(const uint32_t* sorted_keys, size_t n, uint32_t* uniq, uint32_t* first,
+                  uint32_t* count, DevBuf& scratch, cudaStream_t st, size_t* launches) {
+  if (n == 0) return 0;
+  const size_t K = count_runs(sorted_keys, n, scratch, st);
+  emit_runs(sorted_keys, n, K, uniq, first, count, scratch, st);
+  if (launches) *launches += 4;
+  return K;
+}
+
+size_t build_runs(const uint32_t* sorted_keys, size_t n, DevBuf& uniq, DevBuf& first, DevBuf& count,
+                  DevBuf& scratch, cudaStream_t st, size_t* launches) {
+  if (n == 0) return 0;
+  const size_t K = count_runs(sorted_keys, n, scratch, st);
+  uniq.reserve(K * sizeof(uint32_t));
+  first.reserve(K * sizeof(uint32_t));
+  count.reserve(K * sizeof(uint32_t));
+  emit_runs(sorted_keys, n, K, uniq.as<uint32_t>(), first.as<uint32_t>(), count.as<uint32_t>(), scratch, st);
   if (launches) *launches += 4;
   return K;
 }
