@@ -65,14 +65,6 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
-def shard(items, rank, world):
-    """Contiguous near-equal share of items for this rank (replica sharding)."""
-    n = len(items)
-    lo = (n * rank) // world
-    hi = (n * (rank + 1)) // world
-    return items[lo:hi]
-
-
 def init_group(world, backend):
     if world <= 1:
         return None

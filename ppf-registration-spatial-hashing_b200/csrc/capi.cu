@@ -107,18 +107,8 @@ LookupOut finish_lookup(Context& ctx, Model& m, LookupState& st, const SceneData
   if (m.cpu_clustering) {
     float poses[48];
     uint32_t votes[3];
-    int nc = 0;
-    if (ctx.host_greedy) {
-      std::vector<float> T(U * 16);
-      std::vector<uint32_t> cnt(U);
-      PPF_CUDA(cudaMemcpyAsync(T.data(), st.transforms.ptr, U * 64, cudaMemcpyDeviceToHost, ctx.stream));
-      PPF_CUDA(cudaMemcpyAsync(cnt.data(), st.counts.ptr, U * 4, cudaMemcpyDeviceToHost, ctx.stream));
-      PPF_CUDA(cudaStreamSynchronize(ctx.stream));
-      nc = cluster_poses_cpu(T.data(), cnt.data(), U, m.t.d_dist, PPF_D_ANGLE_HOST, poses, votes);
-    } else {
-      nc = cluster_poses_greedy_gpu(ctx, st.transforms.as<float>(), st.counts.as<uint32_t>(), U, m.t.d_dist,
-                                    PPF_D_ANGLE_HOST, poses, votes);
-    }
+    const int nc = cluster_poses_greedy_gpu(ctx, st.transforms.as<float>(), st.counts.as<uint32_t>(), U,
+                                            m.t.d_dist, PPF_D_ANGLE_HOST, poses, votes);
     st.cpu_poses.assign(poses, poses + 16 * nc);
     if (nc > 0) std::memcpy(out.pose, poses, sizeof(out.pose));
     out.stats.max_idx = 0;
@@ -223,7 +213,6 @@ void init_context(Context& c, int device) {
   PPF_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device));
   c.vote_smem_limit = optin - 2048;  // static shared memory of the vote kernel
   if (const char* e = std::getenv("PPF_B200_CHECKS")) c.checks = e[0] == '1';
-  if (const char* e = std::getenv("PPF_B200_HOST_GREEDY")) c.host_greedy = e[0] == '1';
   if (const char* e = std::getenv("PPF_B200_CLUSTER_SPLIT")) c.cluster_split = e[0] != '0';
   if (const char* e = std::getenv("PPF_B200_ENTRY_ORDER")) c.entry_spread = std::strcmp(e, "hash") != 0;
   // test hooks: the n-th device allocation from now fails; the next 32-bit

@@ -53,7 +53,6 @@ struct Context {
   int vote_smem_limit = 0;  // max dynamic shared memory per vote block
   size_t launches = 0;      // kernels launched (running total)
   bool checks = false;      // self-checking kernels (PPF_B200_CHECKS=1)
-  bool host_greedy = false; // cpu_clustering on the host (PPF_B200_HOST_GREEDY=1)
   bool cluster_split = true; // exact-sum split clustering allowed (PPF_B200_CLUSTER_SPLIT=0: never)
   // vote entry order of models built on this context: spread (default) or by
   // m_r then a pair hash (PPF_B200_ENTRY_ORDER=hash)
@@ -233,10 +232,6 @@ int cluster_poses_greedy_gpu(Context& ctx, const float* transforms_dev, const ui
 
 int cluster_poses_sorted_gpu(Context& ctx, const float* transforms_dev, const uint32_t* votes_dev, size_t U,
                              float trans_thresh, float rot_thresh, float out_poses[3 * 16], uint32_t out_votes[3]);
-
-// ---- greedy CPU clustering (cpu_cluster.cpp)
-int cluster_poses_cpu(const float* poses, const uint32_t* votes, size_t n, float trans_thresh,
-                      float rot_thresh, float out_poses[3 * 16], uint32_t out_votes[3]);
 
 }  // namespace ppf
 

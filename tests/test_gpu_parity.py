@@ -309,9 +309,10 @@ def test_candidate_buffer_growth(pkg, ctx, monkeypatch):
     assert _same(pose, pose_ref)
 
 
-def test_gpu_greedy_clustering_equals_host(pkg, ctx, oracle, monkeypatch):
+def test_gpu_greedy_clustering_equals_host(pkg, ctx, oracle):
     """cpu_clustering=True runs the greedy clustering on the device; its best
-    pose and vote total equal the host restatement's on the same kept votes."""
+    pose and vote total equal the oracle's host restatement on the same kept
+    votes."""
     thr = 0.3
     spec = pkg.synthetic.config_plain(seed=141, n_model=1200, n_plane=2500, n_box=800)
     m, s, d = spec.models[0], spec.scene, spec.d_dists[0]
@@ -323,10 +324,6 @@ def test_gpu_greedy_clustering_equals_host(pkg, ctx, oracle, monkeypatch):
     out, votes = oracle.cluster_poses(T, counts, d, 2 * np.float32(np.pi) / 30)
     assert np.array_equal(pose, out[0])
     assert model.stats["best_score"] == float(votes[0])
-    monkeypatch.setenv("PPF_B200_HOST_GREEDY", "1")
-    hctx = pkg.Context(0)
-    hm = pkg.Model(m, d, thr, cpu_clustering=True, context=hctx)
-    assert np.array_equal(hm.ppf_lookup(pkg.Scene(s, d, 5, context=hctx)), pose)
 
 
 def test_gpu_greedy_clustering_many_poses(pkg, ctx, oracle):

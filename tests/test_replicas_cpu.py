@@ -1,7 +1,7 @@
 """The multi-GPU form of bench.py is replicas only: every rank registers its
 own copy of the workload, with no collective on the data path; the timed
-region ends with a max over ranks.  Two gloo ranks on the CPU check the
-sharding helper and the max-over-ranks reduction."""
+region ends with a barrier and a max over ranks.  Two gloo ranks on the CPU
+run bench.py's process-group set-up, barrier and max-over-ranks reduction."""
 import os
 import socket
 
@@ -21,21 +21,24 @@ def _rank(rank, world, port, out):
     import bench
 
     dist = bench.init_group(world, "gloo")
-    items = list(range(11))
-    mine = bench.shard(items, rank, world)
+    dist.barrier()
     t = bench.reduce_max(dist, 1.5 + rank)
-    out[rank] = (mine, t)
+    out[rank] = t
     dist.destroy_process_group()
 
 
-def test_two_gloo_ranks_shard_and_max():
+def test_two_gloo_ranks_barrier_and_max():
     world = 2
     port = _free_port()
     with mp.Manager() as mgr:
         out = mgr.dict()
         mp.spawn(_rank, args=(world, port, out), nprocs=world, join=True)
         res = dict(out)
-    shards = [res[r][0] for r in range(world)]
-    assert sorted(sum(shards, [])) == list(range(11))
-    assert all(abs(len(a) - len(b)) <= 1 for a in shards for b in shards)
-    assert all(res[r][1] == pytest.approx(1.5 + world - 1) for r in range(world))
+    assert all(res[r] == pytest.approx(1.5 + world - 1) for r in range(world))
+    assert bench_single_rank_is_identity()
+
+
+def bench_single_rank_is_identity():
+    import bench
+
+    return bench.init_group(1, "gloo") is None and bench.reduce_max(None, 2.5) == 2.5
