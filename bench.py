@@ -289,10 +289,22 @@ def run_cpu_config1(args):
           flush=True)
 
 
+SERVE_PRESETS = {
+    # name: (models, model point range, scene point range, scenes, workers, seed)
+    "small": (8, (2000, 6000), (5000, 40000), 64, 4, 1003),
+    # 16 models of 2k-20k points, scenes of 5k-200k points
+    # (the first --serve-scenes of its 256 scenes)
+    "config3": (16, (2000, 20000), (5000, 200000), 24, 2, 1002),
+    # 64 models of 2k-20k points, scenes of 5k-300k points
+    "config4": (64, (2000, 20000), (5000, 300000), 16, 2, 1005),
+}
+
+
 def run_serve(args):
-    """Library workload: 8 models (2k-6k points by default, tau_d = 0.04),
-    scenes (5k-40k points by default) each holding 1-4 of them; a request
-    registers one scene against the models it holds (ref_point_df=5,
+    """Library workload: --serve-preset small (8 models of 2k-6k points,
+    scenes of 5k-40k points), config3 or config4 (BASELINE's library sizes,
+    on the first --serve-scenes scenes); tau_d = 0.04, each scene holds 1-4
+    library models and a request registers it against them (ref_point_df=5,
     threshold 0.3).
 
     plain  : one ppf_registration per request, rebuilding its models (the
@@ -305,9 +317,11 @@ def run_serve(args):
     import threading
 
     pkg = ge.load_package()
+    n_models, model_range, scene_range, n_scenes, workers, seed = SERVE_PRESETS[args.serve_preset]
+    n_scenes = args.serve_scenes or n_scenes
+    workers = args.serve_workers or workers
     models, d_dists, scenes = pkg.synthetic.config_library(
-        seed=1003, n_models=8, n_scenes=args.serve_scenes, model_range=tuple(args.serve_model_range),
-        scene_range=tuple(args.serve_scene_range))
+        seed=seed, n_models=n_models, n_scenes=n_scenes, model_range=model_range, scene_range=scene_range)
     ctx = pkg.Context(0)
     reqs = [(sc, sorted({i.model_index for i in inst})) for sc, inst in scenes]
     n_reg = sum(len(ids) for _, ids in reqs)
@@ -344,7 +358,7 @@ def run_serve(args):
     ctx.synchronize()
     t_batch = time.perf_counter() - t0
 
-    srv = pkg.Server(lib, workers=args.serve_workers, max_batch=args.serve_max_batch)
+    srv = pkg.Server(lib, workers=workers, max_batch=args.serve_max_batch)
     for t in [srv.submit(sc, ids, REF_DF) for sc, ids in reqs[:4]]:
         srv.wait(t, raise_on_no_votes=False)
 
@@ -375,6 +389,7 @@ def run_serve(args):
 
     light = serve_at(0.7, 7)
     heavy = serve_at(1.5, 8)
+    nominal = serve_at(50.0 * t_batch / len(reqs), 9) if args.serve_preset == "config4" else None
     srv.close()
     line = {"mode": "serve", "metric": METRIC, "unit": METRIC, "higher_is_better": True, "n_gpus": 1,
             "plain": n_reg / t_plain, "batched": n_reg / t_batch, "served": heavy["registrations_per_s"],
@@ -382,13 +397,75 @@ def run_serve(args):
             "served_over_plain": heavy["registrations_per_s"] / (n_reg / t_plain),
             "served_at_70pct": light, "served_at_150pct": heavy,
             "requests": len(reqs), "registrations": n_reg, "data": "synthetic", "dtype": "f32",
-            "config": {"workload": f"library of 8 models ({args.serve_model_range[0]}-{args.serve_model_range[1]} "
-                                   f"pts, tau_d=0.04), {len(reqs)} scenes of {args.serve_scene_range[0]}-"
-                                   f"{args.serve_scene_range[1]} pts holding 1-4 models each, ref_point_df=5, "
-                                   "threshold 0.3",
-                       "served": f"{args.serve_workers} workers, max_batch {args.serve_max_batch}, Poisson arrivals "
-                                 "at 70% and 150% of the batched rate"}}
+            "scene_points_total": int(sum(len(sc) for sc, _ in reqs)),
+            "config": {"preset": args.serve_preset,
+                       "workload": f"library of {n_models} models ({model_range[0]}-{model_range[1]} pts, "
+                                   f"tau_d=0.04), {len(reqs)} scenes of {scene_range[0]}-{scene_range[1]} pts "
+                                   "holding 1-4 models each, ref_point_df=5, threshold 0.3",
+                       "served": f"{workers} workers, max_batch {args.serve_max_batch}, Poisson arrivals at 70% "
+                                 "and 150% of the batched rate"}}
+    if nominal:
+        line["served_at_50_requests_per_s"] = nominal
     print(json.dumps(line), flush=True)
+
+
+def run_large(args):
+    """BASELINE config 5, the large stress case: a 40000-point model (dense
+    superellipsoid + torus union, 1.6e9 ordered pairs in its hash array)
+    against a 1M-point scene holding 10 instances (40% occlusion, plane and box
+    clutter, sigma 1 mm), tau_d 0.025, threshold 0.3.  The model is built in
+    full and timed.  The lookup runs at --large-ref-df (default 1000: 1000 of
+    the 200000 scene reference points that ref_point_df 5 gives); its votes
+    and vote time are reported as measured and, scaled by reference points,
+    projected to ref_point_df 5."""
+    import torch
+
+    pkg = ge.load_package()
+    spec = pkg.synthetic.config_large()
+    m, s, d = spec.models[0], spec.scene, spec.d_dists[0]
+    ctx = pkg.Context(0)
+    dev = torch.device("cuda", 0)
+    free0, total = torch.cuda.mem_get_info(dev)
+    md = (torch.from_numpy(m.points).to(dev), torch.from_numpy(m.normals).to(dev))
+    sd = (torch.from_numpy(s.points).to(dev), torch.from_numpy(s.normals).to(dev))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    model = pkg.Model(md, d, THR, context=ctx)
+    ctx.synchronize()
+    build_s = time.perf_counter() - t0
+    free_build = torch.cuda.mem_get_info(dev)[0]
+    scene = pkg.Scene(sd, d, args.large_ref_df, context=ctx)
+    t0 = time.perf_counter()
+    pose = model.ppf_lookup(scene, raise_on_no_votes=False)
+    ctx.synchronize()
+    lookup_s = time.perf_counter() - t0
+    st = dict(model.stats)
+    free_lookup = torch.cuda.mem_get_info(dev)[0]
+    n_ref = (len(s) + args.large_ref_df - 1) // args.large_ref_df
+    n_ref5 = (len(s) + 4) // 5
+    scale = n_ref5 / n_ref
+    best = min(((float(np.linalg.norm(pose[:3, 3] - i.pose[:3, 3])) / spec.diameters[0],
+                 float(np.degrees(np.arccos(np.clip((np.trace(pose[:3, :3].T @ i.pose[:3, :3]) - 1) / 2, -1, 1)))))
+                for i in spec.instances), key=lambda e: e[0])
+    # the model build's two radix sorts: 4 passes of 32-bit keys + 32-bit
+    # values and 8 passes of 64-bit keys + 32-bit values, each pass reading
+    # and writing every element once
+    P = len(m) ** 2
+    sort_bytes = P * (4 * 2 * (4 + 4) + 8 * 2 * (8 + 4))
+    print(json.dumps({
+        "mode": "large", "workload": f"config 5: {len(m)}-pt model ({P:.3g} pairs), {len(s)}-pt scene with "
+                                     f"{len(spec.instances)} instances, tau_d 0.025, threshold 0.3",
+        "model_build_s": build_s, "model_keys": int(pkg.api._lib().ppf_model_num_keys(model.handle)),
+        "num_chunks": model.num_chunks, "sort_algorithmic_bytes": sort_bytes,
+        "ref_point_df": args.large_ref_df, "scene_ref_points": n_ref, "lookup_s": lookup_s,
+        "n_votes": st["n_votes"], "vote_ms": st["vote_ms"], "total_ms": st["total_ms"],
+        "votes_per_s": st["n_votes"] / (st["vote_ms"] / 1000.0) if st["vote_ms"] else None,
+        "n_kept": st["n_kept"], "n_candidates": st["n_candidates"], "max_vote_count": st["max_vote_count"],
+        "projected_ref_point_df5": {"scene_ref_points": n_ref5, "n_votes": st["n_votes"] * scale,
+                                    "vote_s": st["vote_ms"] / 1000.0 * scale},
+        "device_memory_used_gb": {"after_build": (free0 - free_build) / 1e9,
+                                  "after_lookup": (free0 - free_lookup) / 1e9, "total": total / 1e9},
+        "nearest_instance_err_terr_over_diam_deg": best}), flush=True)
 
 
 def run_profile_case(args):
@@ -437,15 +514,16 @@ def main():
     ap.add_argument("--serve", action="store_true",
                     help="library workload: plain per-request registration vs batched lookups vs the "
                          "request loop under Poisson arrivals (p50/p99 latency)")
-    ap.add_argument("--serve-scenes", type=int, default=64)
-    ap.add_argument("--serve-model-range", type=int, nargs=2, default=(2000, 6000))
-    ap.add_argument("--serve-scene-range", type=int, nargs=2, default=(5000, 40000))
-    ap.add_argument("--serve-workers", type=int, default=4)
+    ap.add_argument("--serve-preset", default="small", choices=sorted(SERVE_PRESETS))
+    ap.add_argument("--serve-scenes", type=int, default=0, help="scenes (requests); 0: the preset's")
+    ap.add_argument("--serve-workers", type=int, default=0, help="request-loop workers; 0: the preset's")
     ap.add_argument("--serve-max-batch", type=int, default=16)
     ap.add_argument("--profile-case", action="store_true",
                     help="one lookup of one model at ref_point_df=50 (short vote launch for ncu)")
     ap.add_argument("--profile-model", type=int, default=0)
     ap.add_argument("--profile-all", action="store_true", help="the profile case of each of the four models")
+    ap.add_argument("--large", action="store_true", help="config 5 (40k-point model, 1M-point scene), sampled lookup")
+    ap.add_argument("--large-ref-df", type=int, default=1000)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -455,6 +533,8 @@ def main():
         return run_profile_case(args)
     if args.serve:
         return run_serve(args)
+    if args.large:
+        return run_large(args)
 
     import torch
 
