@@ -69,8 +69,11 @@ int ppf_abi_version(void);
  * (src/cuda/ppf.cu:37-49).  The context owns a CUDA stream and a workspace;
  * it never resets the device (the reference calls cudaDeviceReset at the end
  * of ppf_registration, src/cuda/ppf.cu:103).  Models and scenes keep using
- * the context that made them, up to and including their destroy call:
- * destroy them (and any server over them) before the context. */
+ * the context that made them; each holds a reference on it, and a server
+ * holds one on each of its library models.  Handles may be destroyed in any
+ * order: ppf_context_destroy and ppf_model_destroy drop the caller's
+ * reference, and the context or model goes (after its stream finishes) when
+ * the last model, scene or server using it is destroyed. */
 ppf_status ppf_context_create(int device, ppf_context_t* out);
 ppf_status ppf_context_destroy(ppf_context_t ctx);
 ppf_status ppf_context_synchronize(ppf_context_t ctx);
@@ -170,8 +173,9 @@ ppf_status ppf_voxel_downsample(ppf_context_t ctx, const float* xyz, const float
 
 /* Request loop over a resident model library: a serving form of
  * ppf_registration (src/cuda/ppf.cu:29-106), which instead rebuilds every
- * model for every call.  The models stay owned by the caller and must
- * outlive the server.  n_workers threads, each with its own context on
+ * model for every call.  The server holds a reference on each library
+ * model until ppf_server_destroy, so the caller may destroy its model handles
+ * earlier.  n_workers threads, each with its own context on
  * `device`, take queued requests in arrival order and admit them while their
  * estimated device memory (scene, candidate cells, lookup state) fits
  * memory_budget bytes; up to max_batch admitted requests share one batched

@@ -56,6 +56,29 @@ ppf_status guarded(F&& f) {
   }
 }
 
+// Reference counts of the handles (see engine.h): releasing the last
+// reference waits for the object's stream and frees it.
+void release_context(ppf_context_s* c) {
+  if (c && c->refs.fetch_sub(1) == 1) {
+    cudaSetDevice(c->c.device);
+    cudaStreamSynchronize(c->c.stream);
+    delete c;
+  }
+}
+
+void release_model(ppf_model_s* m) {
+  if (m && m->refs.fetch_sub(1) == 1) {
+    ppf_context_s* owner = m->owner;
+    {
+      cudaSetDevice(m->m.ctx->device);
+      StreamScope scope(m->m.ctx->stream);
+      cudaStreamSynchronize(m->m.ctx->stream);
+      delete m;
+    }
+    release_context(owner);
+  }
+}
+
 void copy_out(void* dst, const void* src_dev, size_t bytes, cudaStream_t st) {
   if (!dst || !bytes) return;
   PPF_CUDA(cudaMemcpyAsync(dst, src_dev, bytes, cudaMemcpyDefault, st));
@@ -214,7 +237,6 @@ void init_context(Context& c, int device) {
   c.vote_smem_limit = optin - 2048;  // static shared memory of the vote kernel
   if (const char* e = std::getenv("PPF_B200_CHECKS")) c.checks = e[0] == '1';
   if (const char* e = std::getenv("PPF_B200_CLUSTER_SPLIT")) c.cluster_split = e[0] != '0';
-  if (const char* e = std::getenv("PPF_B200_ENTRY_ORDER")) c.entry_spread = std::strcmp(e, "hash") != 0;
   // test hooks: the n-th device allocation from now fails; the next 32-bit
   // radix sort on this context has one tile withhold its look-back status,
   // so that the tiles waiting on it give up after a short bounded spin
@@ -249,11 +271,7 @@ ppf_status ppf_context_create(int device, ppf_context_t* out) {
 
 ppf_status ppf_context_destroy(ppf_context_t ctx) {
   return guarded([&]() {
-    if (ctx) {
-      cudaSetDevice(ctx->c.device);
-      cudaStreamSynchronize(ctx->c.stream);
-      delete ctx;
-    }
+    release_context(ctx);
     return PPF_OK;
   });
 }
@@ -287,6 +305,8 @@ ppf_status ppf_model_create(ppf_context_t ctx, const float* xyz, const float* nx
     m->m.use_l1_norm = use_l1_norm != 0;
     m->m.use_averaged_clusters = use_averaged_clusters != 0;
     build_model(ctx->c, m->m.t, xyz, nxyz, n, d_dist);
+    m->owner = ctx;
+    ctx->refs.fetch_add(1);
     *out = m.release();
     return PPF_OK;
   });
@@ -307,12 +327,7 @@ ppf_status ppf_model_set_point_vote_weights(ppf_model_t m, const float* w, uint6
 
 ppf_status ppf_model_destroy(ppf_model_t m) {
   return guarded([&]() {
-    if (m) {
-      cudaSetDevice(m->m.ctx->device);
-      StreamScope scope(m->m.ctx->stream);
-      cudaStreamSynchronize(m->m.ctx->stream);
-      delete m;
-    }
+    release_model(m);
     return PPF_OK;
   });
 }
@@ -338,6 +353,8 @@ ppf_status ppf_scene_create(ppf_context_t ctx, const float* xyz, const float* nx
     s->s.ref_df = ref_point_df ? ref_point_df : 1;
     upload_points(ctx->c, xyz, n, s->s.pts);
     upload_points(ctx->c, nxyz, n, s->s.nrm);
+    s->owner = ctx;
+    ctx->refs.fetch_add(1);
     *out = s.release();
     return PPF_OK;
   });
@@ -346,10 +363,14 @@ ppf_status ppf_scene_create(ppf_context_t ctx, const float* xyz, const float* nx
 ppf_status ppf_scene_destroy(ppf_scene_t s) {
   return guarded([&]() {
     if (s) {
-      cudaSetDevice(s->ctx->device);
-      StreamScope scope(s->ctx->stream);
-      cudaStreamSynchronize(s->ctx->stream);
-      delete s;
+      ppf_context_s* owner = s->owner;
+      {
+        cudaSetDevice(s->ctx->device);
+        StreamScope scope(s->ctx->stream);
+        cudaStreamSynchronize(s->ctx->stream);
+        delete s;
+      }
+      release_context(owner);
     }
     return PPF_OK;
   });
@@ -506,6 +527,11 @@ ppf_status ppf_server_create(int device, uint64_t n_models, const ppf_model_t* m
     }
     std::unique_ptr<ppf_server_s> s(new ppf_server_s());
     s->srv = server_create(device, ms, memory_budget, n_workers, max_batch);
+    // the server holds each library model (and through it its context)
+    for (uint64_t j = 0; j < n_models; ++j) {
+      models[j]->refs.fetch_add(1);
+      s->library.push_back(models[j]);
+    }
     *out = s.release();
     return PPF_OK;
   });
@@ -537,6 +563,7 @@ ppf_status ppf_server_destroy(ppf_server_t srv) {
   return guarded([&]() {
     if (srv) {
       if (srv->srv) server_destroy(srv->srv);
+      for (ppf_model_s* m : srv->library) release_model(m);
       delete srv;
     }
     return PPF_OK;
@@ -558,11 +585,12 @@ ppf_status ppf_registration(ppf_context_t ctx, uint64_t n_scenes, const float* c
                 PPF_ERR_INVALID_ARGUMENT, "null model arrays");
     PPF_REQUIRE(n_scenes == 0 || (scene_xyz && scene_nxyz && scene_n), PPF_ERR_INVALID_ARGUMENT,
                 "null scene arrays");
-    std::unique_ptr<ppf_context_s> own;
+    std::unique_ptr<ppf_context_s, void (*)(ppf_context_s*)> own(nullptr, release_context);
     ppf_context_t c = ctx;
     if (!c) {
-      own.reset(new ppf_context_s());
-      init_context(own->c, dev_use);
+      std::unique_ptr<ppf_context_s> fresh(new ppf_context_s());
+      init_context(fresh->c, dev_use);
+      own.reset(fresh.release());
       c = own.get();
     }
     PPF_CUDA(cudaSetDevice(c->c.device));

@@ -2,6 +2,7 @@
 // resident scenes, and the device-side layout the kernels consume.
 #pragma once
 
+#include <atomic>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -25,11 +26,8 @@ constexpr int kVoteWarps = kVoteThreads / 32;
 // segment offset (+1 entry).
 constexpr int kVoteQueueBytes = kVoteThreads * (4 + 4 + 4 + 8) + (kVoteThreads + 4) * 4;
 // Accumulator words of a chunk: one 32-bit counter per (m_r, alpha bin) cell
-// (the reference counts votes in unsigned int too, include/impl/util.hpp:30-52),
-// row_stride words per m_r row (kBins, or 32 with the spread entry order).
-inline size_t vote_acc_words(uint32_t chunk, uint32_t row_stride) {
-  return ((size_t)chunk * row_stride + 3) & ~size_t(3);
-}
+// (the reference counts votes in unsigned int too, include/impl/util.hpp:30-52).
+inline size_t vote_acc_words(uint32_t chunk) { return ((size_t)chunk * kBins + 3) & ~size_t(3); }
 // Angle quantum on the host (include/kernel.h:16 evaluated in float).
 #define PPF_D_ANGLE_HOST ((2.0f * 3.141592654f) / float(30))
 
@@ -54,9 +52,6 @@ struct Context {
   size_t launches = 0;      // kernels launched (running total)
   bool checks = false;      // self-checking kernels (PPF_B200_CHECKS=1)
   bool cluster_split = true; // exact-sum split clustering allowed (PPF_B200_CLUSTER_SPLIT=0: never)
-  // vote entry order of models built on this context: spread (default) or by
-  // m_r then a pair hash (PPF_B200_ENTRY_ORDER=hash)
-  bool entry_spread = true;
   ~Context();
 };
 
@@ -85,9 +80,6 @@ struct ModelTables {
   uint32_t ht_mask = 0;
   // m_r chunking of the vote accumulator
   uint32_t chunk = 0, n_chunks = 0;
-  // accumulator words per m_r row: 32 for the spread entry order (bank =
-  // bin), kBins for the m_r-then-hash order
-  uint32_t row_stride = kBins;
   DevBuf split;  // uint32 [K * (n_chunks + 1)] first run position per chunk
 };
 
@@ -235,16 +227,26 @@ int cluster_poses_sorted_gpu(Context& ctx, const float* transforms_dev, const ui
 
 }  // namespace ppf
 
+// Handles are reference-counted: the caller's handle is one reference, and
+// every model, scene and server made on a context holds one on it (a server
+// also holds one on each library model).  A destroy call drops the caller's
+// reference; the object goes when the last one does, so handles can be
+// destroyed in any order.
 struct ppf_context_s {
   ppf::Context c;
+  std::atomic<int> refs{1};
 };
 struct ppf_model_s {
   ppf::Model m;
+  ppf_context_s* owner = nullptr;
+  std::atomic<int> refs{1};
 };
 struct ppf_scene_s {
   ppf::Context* ctx = nullptr;
+  ppf_context_s* owner = nullptr;
   ppf::SceneData s;
 };
 struct ppf_server_s {
   ppf::Server* srv = nullptr;
+  std::vector<ppf_model_s*> library;
 };

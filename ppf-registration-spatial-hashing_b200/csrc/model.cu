@@ -70,56 +70,6 @@ __global__ void order_words_kernel(const uint32_t* __restrict__ keys, const uint
   }
 }
 
-// Spread vote order, step 1: by key, then m_r chunk, then the 21-bit angle
-// beta_m of u (the pair's second point in the frame of the first).  Chunk
-// indices fit 10 bits (a chunk holds at least 64 of at most 65535 points).
-__global__ void order_words_spread_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ pairs,
-                                          size_t P, uint32_t n, uint32_t chunk, const float4* __restrict__ pts,
-                                          const float4* __restrict__ r1, const float4* __restrict__ r2,
-                                          unsigned long long* __restrict__ words) {
-  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < P;
-       j += (size_t)gridDim.x * blockDim.x) {
-    const uint32_t pr = pairs[j];
-    const uint32_t mr = pr / n, mi = pr - mr * n;
-    FrameYZ f;
-    f.r1 = r1[mr];
-    f.r2 = r2[mr];
-    const float4 q4 = pts[mi];
-    const uint32_t beta = angle21(frame_point_yz(f, make_float3(q4.x, q4.y, q4.z)));
-    words[j] = ((unsigned long long)keys[j] << 32) | ((unsigned long long)(mr / chunk) << PPF_ANGLE_BITS) | beta;
-  }
-}
-
-// Spread vote order, step 2: inside each (run, chunk) sub-run, whose entries
-// step 1 sorted by beta_m, entry i of L goes to position
-// w*q + min(w, L mod W) + i / W with W = ceil(L / 32), w = i mod W and
-// q = L / W: consecutive positions take every W-th angle, so the 32 entries a
-// warp counts together spread over the sub-run's angles.  For one scene
-// pair the bin of a vote is (scene angle - beta_m) in 30ths of a turn, and
-// with 32-word accumulator rows a counter's shared-memory bank is its bin,
-// so a warp's 32 atomics meet few bank conflicts.  A bijection on each
-// sub-run: the chunk boundaries (split) stay valid.
-__global__ void deal_kernel(const uint32_t* __restrict__ epairs_in, size_t P, uint32_t n, uint32_t chunk,
-                            uint32_t n_chunks, const uint32_t* __restrict__ first, size_t K,
-                            const uint32_t* __restrict__ split, uint32_t* __restrict__ epairs_out) {
-  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < P;
-       j += (size_t)gridDim.x * blockDim.x) {
-    const uint32_t pr = epairs_in[j];
-    const uint32_t c = (pr / n) / chunk;
-    size_t lo = 0, hi = K;  // run of position j: last run start <= j
-    while (hi - lo > 1) {
-      const size_t mid = (lo + hi) >> 1;
-      if (first[mid] <= j) lo = mid;
-      else hi = mid;
-    }
-    const uint32_t* sp = split + lo * (n_chunks + 1);
-    const uint32_t s0 = sp[c], L = sp[c + 1] - s0;
-    const uint32_t i = (uint32_t)j - s0;
-    const uint32_t W = (L + 31) / 32, w = i % W, l = i / W, q = L / W, rmd = L % W;
-    epairs_out[(size_t)s0 + w * q + min(w, rmd) + l] = pr;
-  }
-}
-
 // Vote entry of each pair in vote order: (m_r mod chunk) << 21 | angle21(u),
 // u = the pair's second point in the frame of the first: the top 11 bits are
 // the pair's m_r inside its chunk, so the vote kernel forms the cell index
@@ -177,7 +127,7 @@ __global__ void ht_build_kernel(const uint32_t* __restrict__ uniq, size_t K, uin
 }
 
 // split[r*(C+1) + c] = first position of run r whose m_r >= c*chunk
-// (entries of a run are in chunk order).
+// (entries of a run are in m_r order).
 __global__ void split_kernel(const uint32_t* __restrict__ epairs, uint32_t n,
                              const uint32_t* __restrict__ first,
                              const uint32_t* __restrict__ count, size_t K, uint32_t chunk,
@@ -345,10 +295,9 @@ void build_model(Context& ctx, ModelTables& t, const float* xyz, const float* nx
   t.K = build_runs(t.keys.as<uint32_t>(), t.P, t.uniq, t.first, t.count, ctx.scratch, st, &ctx.launches);
 
   // m_r chunks sized to the vote kernel's shared-memory accumulator
-  t.row_stride = ctx.entry_spread ? 32u : (uint32_t)kBins;
   uint32_t max_chunk = 64;
   // (m_r mod chunk fits the 11 bits above an entry's 21-bit angle)
-  while (vote_acc_words(max_chunk + 1, t.row_stride) * 4 + kVoteQueueBytes <= (size_t)ctx.vote_smem_limit &&
+  while (vote_acc_words(max_chunk + 1) * 4 + kVoteQueueBytes <= (size_t)ctx.vote_smem_limit &&
          max_chunk < (1u << (32 - PPF_ANGLE_BITS)))
     ++max_chunk;
   t.n_chunks = (t.n + max_chunk - 1) / max_chunk;
@@ -363,13 +312,8 @@ void build_model(Context& ctx, ModelTables& t, const float* xyz, const float* nx
   {
     DevBuf words;
     words.reserve(t.P * sizeof(unsigned long long));
-    if (t.row_stride == 32u)
-      order_words_spread_kernel<<<grid_for(t.P, 256), 256, 0, st>>>(
-          t.keys.as<uint32_t>(), t.pairs.as<uint32_t>(), t.P, t.n, t.chunk, t.pts.as<float4>(),
-          t.frame_r1.as<float4>(), t.frame_r2.as<float4>(), words.as<unsigned long long>());
-    else
-      order_words_kernel<<<grid_for(t.P, 256), 256, 0, st>>>(t.keys.as<uint32_t>(), t.pairs.as<uint32_t>(),
-                                                              t.P, t.n, words.as<unsigned long long>());
+    order_words_kernel<<<grid_for(t.P, 256), 256, 0, st>>>(t.keys.as<uint32_t>(), t.pairs.as<uint32_t>(),
+                                                            t.P, t.n, words.as<unsigned long long>());
     PPF_CUDA(cudaMemcpyAsync(t.epairs.ptr, t.pairs.ptr, t.P * 4, cudaMemcpyDeviceToDevice, st));
     PPF_CUDA(cudaGetLastError());
     size_t l1 = ctx.sort64.launches();
@@ -382,17 +326,6 @@ void build_model(Context& ctx, ModelTables& t, const float* xyz, const float* nx
                                                       t.split.as<uint32_t>());
     PPF_CUDA(cudaGetLastError());
     ctx.launches++;
-    if (t.row_stride == 32u) {
-      // the sorted pair indices are dealt into the spread order; the sorted
-      // order words are no longer needed, so their buffer holds the result
-      uint32_t* dealt = reinterpret_cast<uint32_t*>(words.ptr);
-      deal_kernel<<<grid_for(t.P, 256), 256, 0, st>>>(t.epairs.as<uint32_t>(), t.P, t.n, t.chunk, t.n_chunks,
-                                                       t.first.as<uint32_t>(), t.K, t.split.as<uint32_t>(),
-                                                       dealt);
-      PPF_CUDA(cudaGetLastError());
-      PPF_CUDA(cudaMemcpyAsync(t.epairs.ptr, dealt, t.P * 4, cudaMemcpyDeviceToDevice, st));
-      ctx.launches++;
-    }
     entries_kernel<<<grid_for(t.P, 256), 256, 0, st>>>(
         t.epairs.as<uint32_t>(), t.P, t.n, t.chunk, t.pts.as<float4>(), t.frame_r1.as<float4>(),
         t.frame_r2.as<float4>(), t.first.as<uint32_t>(), t.K, t.entries.as<uint32_t>(),

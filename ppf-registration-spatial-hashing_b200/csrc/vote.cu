@@ -44,7 +44,6 @@ struct VoteArgs {
   const float4* m_r2;
   const float4* m_pts;
   uint32_t n_m, chunk, n_chunks;
-  uint32_t row_stride;  // accumulator words per m_r row
   // scene
   const float4* s_pts;
   const float4* s_nrm;
@@ -100,12 +99,18 @@ __device__ __forceinline__ uint32_t ht_lookup(const uint32_t* __restrict__ keys,
   return kNoRun;
 }
 
-// Block barrier of the vote kernel.  Each warp is gathered (__syncwarp) and
-// its shared-memory stores are fenced before it arrives, and its loads after
-// the barrier are fenced again.  Without the fences the -O3 build of this
-// kernel was seen to let warp 0 fall one barrier phase behind the others on
-// one 60000-point scene (the other warps read the segment scan before warp 0
-// had written it); with them, and with -Xptxas -O1 or -O0, it did not.
+// Block barrier of the vote kernel.  __syncthreads() is an .aligned barrier:
+// every lane of a warp must reach it together.  Each barrier here follows
+// lane-conditional code (lane 31 stores a warp total before the scan
+// barriers, lane 0 stores sh.item, sh.base and the counters), and with
+// independent thread scheduling an optimised build may bring a warp to the
+// barrier in two groups, so that the barrier releases on the first and the
+// rest of the warp runs one barrier phase behind.  That is what a -O3 build
+// without the __syncwarp() did on one 60000-point scene (the other warps
+// read the segment scan before warp 0 had written it; -O1 and -O0 builds
+// did not).
+// __syncwarp() reconverges the warp first; the fences around the barrier
+// order the shared-memory stores and loads on both sides.
 __device__ __forceinline__ void block_sync() {
   __syncwarp();
   __threadfence_block();
@@ -213,8 +218,7 @@ __device__ __forceinline__ void vote_item(const VoteArgs& a, uint32_t slot_of_it
   uint32_t* acc = q_seg + kVoteThreads + 4;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const uint32_t stride = a.row_stride;
-  const uint32_t cells = a.chunk * stride;
+  const uint32_t cells = a.chunk * kBins;
   {
     const uint32_t item = a.item_list ? a.item_list[slot_of_item] : slot_of_item;
     const uint32_t c = item % a.n_chunks;
@@ -330,7 +334,7 @@ __device__ __forceinline__ void vote_item(const VoteArgs& a, uint32_t slot_of_it
             const uint32_t e = __ldg(a.entries + pos);
             const uint32_t y = bsh - (e << kShift);
             if (!(y * (uint32_t)PPF_N_ANGLE - m_lo > m_span)) continue;
-            const uint32_t row = (e >> PPF_ANGLE_BITS) * stride;
+            const uint32_t row = (e >> PPF_ANGLE_BITS) * kBins;
             const uint32_t fast = row + __umulhi(y, (uint32_t)PPF_N_ANGLE);
             const uint32_t exact = row + exact_bin<kCheck>(a, pos, vv);
             if (exact != fast && in_range<kCheck>(a, 7, exact, cells)) {
@@ -343,7 +347,7 @@ __device__ __forceinline__ void vote_item(const VoteArgs& a, uint32_t slot_of_it
         if (bw & kExactOnly) {
           // degenerate frame vector or run: every vote takes the exact path
           for (uint32_t k = lane; k < n_here; k += 32) {
-            const uint32_t row = (__ldg(a.entries + start + k) >> PPF_ANGLE_BITS) * stride;
+            const uint32_t row = (__ldg(a.entries + start + k) >> PPF_ANGLE_BITS) * kBins;
             const uint32_t cell = row + exact_bin<kCheck>(a, start + k, vv);
             if (in_range<kCheck>(a, 6, cell, cells)) atomicAdd(&acc[cell], 1u);
             ++st.exact;
@@ -362,7 +366,7 @@ __device__ __forceinline__ void vote_item(const VoteArgs& a, uint32_t slot_of_it
             for (int u = 0; u < kUnroll; ++u) {
               const uint32_t y = bsh - (c[u] << kShift);
               amb |= y * (uint32_t)PPF_N_ANGLE - m_lo > m_span;
-              c[u] = (c[u] >> PPF_ANGLE_BITS) * stride + __umulhi(y, (uint32_t)PPF_N_ANGLE);
+              c[u] = (c[u] >> PPF_ANGLE_BITS) * kBins + __umulhi(y, (uint32_t)PPF_N_ANGLE);
             }
 #pragma unroll
             for (int u = 0; u < kUnroll; ++u)
@@ -372,9 +376,9 @@ __device__ __forceinline__ void vote_item(const VoteArgs& a, uint32_t slot_of_it
           for (uint32_t k = nfull * 32 * kUnroll + lane; k < n_here; k += 32) {
             const uint32_t e = __ldg(a.entries + start + k);
             const uint32_t y = bsh - (e << kShift);
-            uint32_t cell = (e >> PPF_ANGLE_BITS) * stride + __umulhi(y, (uint32_t)PPF_N_ANGLE);
+            uint32_t cell = (e >> PPF_ANGLE_BITS) * kBins + __umulhi(y, (uint32_t)PPF_N_ANGLE);
             if (y * (uint32_t)PPF_N_ANGLE - m_lo > m_span) {
-              cell = (e >> PPF_ANGLE_BITS) * stride + exact_bin<kCheck>(a, start + k, vv);
+              cell = (e >> PPF_ANGLE_BITS) * kBins + exact_bin<kCheck>(a, start + k, vv);
               ++st.exact;
             }
             if (in_range<kCheck>(a, 8, cell, cells)) atomicAdd(&acc[cell], 1u);
@@ -453,7 +457,7 @@ __device__ __forceinline__ void vote_item(const VoteArgs& a, uint32_t slot_of_it
       for (uint32_t cell = tid; cell < cells; cell += kVoteThreads) {
         const uint32_t cnt = acc[cell];
         if (cnt != 0u && (a.emit_all || (float)cnt > floor_v)) {
-          const uint32_t mr = mr_lo + cell / stride, bin = cell % stride;
+          const uint32_t mr = mr_lo + cell / kBins, bin = cell % kBins;
           if (in_range<kCheck>(a, 10, slot, a.cand_cap)) {
             a.cand_code[slot] = ((unsigned long long)sr << 32) | ((unsigned long long)mr << 6) | bin;
             a.cand_count[slot] = cnt;
@@ -575,7 +579,6 @@ VoteArgs make_args(const Model& m, const SceneData& s) {
   a.n_m = t.n;
   a.chunk = t.chunk;
   a.n_chunks = t.n_chunks;
-  a.row_stride = t.row_stride;
   a.s_pts = s.pts.as<float4>();
   a.s_nrm = s.nrm.as<float4>();
   a.n_s = s.n;
@@ -629,7 +632,7 @@ VoteResult run_votes(Context& ctx, const Model& m, const SceneData& s, bool emit
   a.bad = reinterpret_cast<unsigned long long*>(ctx.flags.as<uint32_t>() + 8);
   auto kernel = check ? vote_kernel<true> : vote_kernel<false>;
 
-  const size_t smem = kVoteQueueBytes + vote_acc_words(a.chunk, a.row_stride) * 4;
+  const size_t smem = kVoteQueueBytes + vote_acc_words(a.chunk) * 4;
   PPF_REQUIRE((int)smem <= ctx.vote_smem_limit, PPF_ERR_INTERNAL, "vote accumulator too large");
   PPF_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   PPF_CUDA(cudaEventRecord(ctx.ev[0], stream));
@@ -721,7 +724,7 @@ void run_votes_batch(Context& ctx, std::vector<BatchVote>& reqs) {
     total += items;
     PPF_REQUIRE(total < 0xffffffffull, PPF_ERR_INVALID_ARGUMENT, "more than 2^32 work items in one batch");
     item_off[i + 1] = (uint32_t)total;
-    smem = std::max(smem, kVoteQueueBytes + vote_acc_words(a0.chunk, a0.row_stride) * 4);
+    smem = std::max(smem, kVoteQueueBytes + vote_acc_words(a0.chunk) * 4);
   }
   PPF_REQUIRE((int)smem <= ctx.vote_smem_limit, PPF_ERR_INTERNAL, "vote accumulator too large");
   ctx.batch_redo.reserve(std::max<size_t>(total, 1) * sizeof(uint32_t));
@@ -804,7 +807,7 @@ void run_votes_batch(Context& ctx, std::vector<BatchVote>& reqs) {
     a.n_items = hc[3];
     a.work_counter = cnt0 + 16 * i + 12;
     PPF_CUDA(cudaMemsetAsync(a.n_redo, 0, 4, stream));
-    const size_t smem_i = kVoteQueueBytes + vote_acc_words(a.chunk, a.row_stride) * 4;
+    const size_t smem_i = kVoteQueueBytes + vote_acc_words(a.chunk) * 4;
     PPF_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_i));
     kernel<<<(unsigned)std::min<size_t>(a.n_items, (size_t)sm_count()), kVoteThreads, smem_i, stream>>>(a);
     PPF_CUDA(cudaGetLastError());
@@ -928,7 +931,7 @@ void vote_cells_noalloc(Context& ctx, const Model& m, const float* xyz, const fl
               std::to_string(n_ref) + " scene reference points x " + std::to_string(m.t.n_chunks) +
                   " model chunks exceed the allocation-free limit of " + std::to_string(kNoAllocMaxItems) +
                   " work items");
-  const size_t smem = kVoteQueueBytes + vote_acc_words(m.t.chunk, m.t.row_stride) * 4;
+  const size_t smem = kVoteQueueBytes + vote_acc_words(m.t.chunk) * 4;
   PPF_REQUIRE((int)smem <= ctx.vote_smem_limit, PPF_ERR_INTERNAL, "vote accumulator too large");
 
   unsigned char* scratch = vote_scratch(ctx.device);

@@ -395,29 +395,6 @@ def test_cluster_path_selection(pkg, ctx):
         assert model.stats["cluster_path"] == path, (kw, w)
 
 
-def test_entry_orders_give_identical_results(pkg, ctx, monkeypatch):
-    """The spread vote-entry order (32-word accumulator rows) and the m_r-then-
-    hash order (31-word rows) count the same votes: identical cells, kept
-    votes, scores and pose, on a model of three chunks."""
-    spec = pkg.synthetic.config_plain(seed=171, n_model=3500, n_plane=2500, n_box=800)
-    m, s, d = spec.models[0], spec.scene, spec.d_dists[0]
-    monkeypatch.setenv("PPF_B200_ENTRY_ORDER", "hash")
-    hctx = pkg.Context(0)
-    a = pkg.Model(m, d, 0.3, context=ctx)
-    b = pkg.Model(m, d, 0.3, context=hctx)
-    assert a.num_chunks == b.num_chunks == 3
-    sa, sb = pkg.Scene(s, d, 5, context=ctx), pkg.Scene(s, d, 5, context=hctx)
-    pa, pb = a.ppf_lookup(sa).copy(), b.ppf_lookup(sb).copy()
-    assert _same(pa, pb)
-    for x, y in zip(a.get_votes(), b.get_votes()):
-        assert np.array_equal(x, y)
-    for x, y in zip(a.get_cluster_state(), b.get_cluster_state()):
-        assert _same(x, y)
-    ca, ka = a.all_votes(sa)
-    cb, kb = b.all_votes(sb)
-    assert np.array_equal(ca, cb) and np.array_equal(ka, kb)
-
-
 def test_cpp_facade_matches_python_api(pkg, ctx, tmp_path):
     """The C++ facade (include/ppf_b200.hpp) registering PLY files, as the
     reference's driver does, gives the poses of the Python API bit for bit."""
