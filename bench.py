@@ -194,7 +194,7 @@ def cpu_sample(orc, O, spec, refs_per_model, offset, threads):
     return time.perf_counter() - t0, proj, done
 
 
-def cpu_baseline(spec, sample_refs=4, threads=None, offset=0):
+def cpu_baseline(spec, sample_refs=2, threads=None, offset=0):
     """The oracle (C++/OpenMP restatement of the reference path) on a bounded
     sample of the workload: every model's hash array in full plus
     `sample_refs` scene reference points per model; the registration rate is
@@ -501,7 +501,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--avg", action="store_true", help="use_averaged_clusters on")
-    ap.add_argument("--cpu-refs", type=int, default=4,
+    ap.add_argument("--cpu-refs", type=int, default=2,
                     help="scene reference points per model in each CPU sample step")
     ap.add_argument("--cpu-config1", action="store_true",
                     help="config 1 registered in full by the CPU oracle (all cores) and a projected 1-core run")
