@@ -153,17 +153,23 @@ def recall_of(spec, poses):
     north star's (translation <= 1% of the model diameter, rotation <= 2 deg)
     and the reference driver's validation (0.1 diameter, 12 deg;
     src/alignment.cpp:300-335)."""
-    errs = []
+    pkg = ge.load_package()
+    families = spec.extra.get("families", [None] * len(spec.models))
+    errs, errs_sym = [], []
     for inst in spec.instances:
         P = poses[inst.model_index]
         G = inst.pose
         terr = float(np.linalg.norm(P[:3, 3] - G[:3, 3])) / spec.diameters[inst.model_index]
-        cosang = (np.trace(P[:3, :3].T @ G[:3, :3]) - 1) / 2
-        errs.append((terr, float(np.degrees(np.arccos(np.clip(cosang, -1, 1))))))
-    strict = sum(t <= 0.01 and a <= 2.0 for t, a in errs)
-    loose = sum(t < 0.1 and a < 12.0 for t, a in errs)
-    return {"terr_over_diam_and_deg": errs, "at_1pct_2deg": f"{strict}/{len(errs)}",
-            "at_reference_bounds_0.1diam_12deg": f"{loose}/{len(errs)}"}
+        errs.append((terr, pkg.synthetic.rotation_error_deg(P[:3, :3], G[:3, :3])))
+        errs_sym.append((terr, pkg.synthetic.rotation_error_deg(P[:3, :3], G[:3, :3], families[inst.model_index])))
+
+    def count(e, t_max, a_max):
+        return f"{sum(t <= t_max and a <= a_max for t, a in e)}/{len(e)}"
+
+    return {"terr_over_diam_and_deg": errs, "at_1pct_2deg": count(errs, 0.01, 2.0),
+            "at_reference_bounds_0.1diam_12deg": count(errs, 0.1, 12.0),
+            "modulo_shape_symmetry": {"terr_over_diam_and_deg": errs_sym, "at_1pct_2deg": count(errs_sym, 0.01, 2.0),
+                                      "at_reference_bounds_0.1diam_12deg": count(errs_sym, 0.1, 12.0)}}
 
 
 def measured_peaks():

@@ -169,6 +169,10 @@ struct VoteShared {
   uint32_t item, next, max, base;
   uint32_t scan_seg[kVoteWarps];   // scratch of the per-tile segment scan
   uint32_t scan_emit[kVoteWarps];  // scratch of the emission scan
+  // q_seg at the first pair of each warp's 32 (q_seg[32 l]), kept
+  // contiguous: the segment search reads all 32 in one conflict-free access
+  // (read in place they sit in one bank, 32 accesses per search)
+  uint32_t seg_blk[kVoteWarps];
   uint32_t wmax[kVoteWarps];       // per-warp maxima of the accumulator
 };
 
@@ -271,6 +275,7 @@ __device__ __forceinline__ void vote_item(const VoteArgs& a, uint32_t slot_of_it
       q_beta[tid] = beta;
       q_v[tid] = v;
       q_seg[tid] = seg0;
+      if (lane == 0) sh.seg_blk[warp] = seg0;
       if (tid == 0) {
         q_seg[kVoteThreads] = n_seg_total;
         sh.next = kVoteWarps;
@@ -287,8 +292,9 @@ __device__ __forceinline__ void vote_item(const VoteArgs& a, uint32_t slot_of_it
       while (s < n_seg_total) {
         // pair p with q_seg[p] <= s < q_seg[p+1]: the last index whose segment
         // offset is <= s (q_seg is nondecreasing and q_seg[0] = 0), found with
-        // two ballots: first over q_seg[32 l], then inside that block of 32
-        const uint32_t blk = 31u - __clz(__ballot_sync(0xffffffffu, q_seg[32 * lane] <= s));
+        // two ballots: first over q_seg[32 l] (its copy seg_blk[l]), then
+        // inside that block of 32
+        const uint32_t blk = 31u - __clz(__ballot_sync(0xffffffffu, sh.seg_blk[lane] <= s));
         const uint32_t plo = 32u * blk + 31u - __clz(__ballot_sync(0xffffffffu, q_seg[32 * blk + lane] <= s));
         const uint32_t p = plo;
         const uint32_t start = q_lo[p] + (s - q_seg[p]) * kSeg;

@@ -42,6 +42,8 @@ __all__ = [
     "config_multi_model",
     "config_library",
     "config_large",
+    "SYMMETRY",
+    "rotation_error_deg",
 ]
 
 
@@ -384,6 +386,45 @@ def occlude(rng, cloud: Cloud, fraction) -> Cloud:
 SHAPES = ("superellipsoid", "torus", "capsules", "spheres_slab")
 
 
+def _rot(axis, angle):
+    c, s_ = np.cos(angle), np.sin(angle)
+    if axis == "x":
+        return np.array([[1, 0, 0], [0, c, -s_], [0, s_, c]])
+    if axis == "y":
+        return np.array([[c, 0, s_], [0, 1, 0], [-s_, 0, c]])
+    return np.array([[c, -s_, 0], [s_, c, 0], [0, 0, 1]])
+
+
+# Rotations (in the model's own frame) that map each shape family onto
+# itself: the superellipsoid's three half-turns, the spheres-on-slab grid's
+# half-turn about z (exact for the slab and the sphere centres; the sphere
+# radii differ, so only approximately for the surface); the torus is
+# symmetric under every rotation about z and a half-turn about x ("axis");
+# the capsule union has none.
+SYMMETRY = {
+    "superellipsoid": [np.eye(3), _rot("x", np.pi), _rot("y", np.pi), _rot("z", np.pi)],
+    "torus": "axis",
+    "capsules": [np.eye(3)],
+    "spheres_slab": [np.eye(3), _rot("z", np.pi)],
+}
+
+
+def rotation_error_deg(R, G, family=None):
+    """Angle in degrees between rotations R and G, or with a shape family the
+    smallest angle over the rotations its symmetry makes equivalent."""
+    R = np.asarray(R, np.float64)
+    G = np.asarray(G, np.float64)
+
+    def ang(A, B):
+        return float(np.degrees(np.arccos(np.clip((np.trace(A.T @ B) - 1) / 2, -1, 1))))
+
+    sym = SYMMETRY.get(family, [np.eye(3)]) if family else [np.eye(3)]
+    if isinstance(sym, str):  # axis symmetry about the model's z
+        c = float(np.clip(abs((R[:, 2]) @ G[:, 2]), -1, 1))
+        return float(np.degrees(np.arccos(c)))
+    return min(ang(R @ S, G) for S in sym)
+
+
 def make_shape(rng, family, n) -> Cloud:
     if family == "superellipsoid":
         return superellipsoid(rng, n)
@@ -488,6 +529,7 @@ def config_multi_model(seed=1001, n_scene=60000, occlusion=0.3, sigma=5e-4, tilt
         diameters=[model_diameter(m) for m in models],
         ref_point_df=ref_point_df,
         vote_count_threshold=vote_count_threshold,
+        extra={"families": list(SHAPES)},
     )
 
 
