@@ -237,7 +237,6 @@ void init_context(Context& c, int device) {
   c.vote_smem_limit = optin - 2048;  // static shared memory of the vote kernel
   if (const char* e = std::getenv("PPF_B200_CHECKS")) c.checks = e[0] == '1';
   if (const char* e = std::getenv("PPF_B200_CLUSTER_SPLIT")) c.cluster_split = e[0] != '0';
-  if (const char* e = std::getenv("PPF_B200_ENTRY_ORDER")) c.entry_order_angle = std::strcmp(e, "angle") == 0;
   // test hooks: the n-th device allocation from now fails; the next 32-bit
   // radix sort on this context has one tile withhold its look-back status,
   // so that the tiles waiting on it give up after a short bounded spin

@@ -52,9 +52,6 @@ struct Context {
   size_t launches = 0;      // kernels launched (running total)
   bool checks = false;      // self-checking kernels (PPF_B200_CHECKS=1)
   bool cluster_split = true; // exact-sum split clustering allowed (PPF_B200_CLUSTER_SPLIT=0: never)
-  // vote entries of a (key, m_r) ordered by angle (PPF_B200_ENTRY_ORDER=angle)
-  // instead of by a hash of the pair index
-  bool entry_order_angle = false;
   ~Context();
 };
 

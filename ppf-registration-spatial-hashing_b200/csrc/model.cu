@@ -70,28 +70,6 @@ __global__ void order_words_kernel(const uint32_t* __restrict__ keys, const uint
   }
 }
 
-// Vote order by key, then m_r, then the top 16 bits of the 21-bit angle
-// beta_m of u (the pair's second point in the frame of the first): the
-// pairs of one (key, m_r) that vote into one (m_r, bin) cell for a scene
-// pair sit next to each other, so a warp's 32 atomics touch fewer distinct
-// cells.  Equal words keep the pair-index order (stable sort).
-__global__ void order_words_angle_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ pairs,
-                                         size_t P, uint32_t n, const float4* __restrict__ pts,
-                                         const float4* __restrict__ r1, const float4* __restrict__ r2,
-                                         unsigned long long* __restrict__ words) {
-  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < P;
-       j += (size_t)gridDim.x * blockDim.x) {
-    const uint32_t pr = pairs[j];
-    const uint32_t mr = pr / n, mi = pr - mr * n;
-    FrameYZ f;
-    f.r1 = r1[mr];
-    f.r2 = r2[mr];
-    const float4 q4 = pts[mi];
-    const uint32_t beta = angle21(frame_point_yz(f, make_float3(q4.x, q4.y, q4.z)));
-    words[j] = ((unsigned long long)keys[j] << 32) | (mr << 16) | (beta >> (PPF_ANGLE_BITS - 16));
-  }
-}
-
 // Vote entry of each pair in vote order: (m_r mod chunk) << 21 | angle21(u),
 // u = the pair's second point in the frame of the first: the top 11 bits are
 // the pair's m_r inside its chunk, so the vote kernel forms the cell index
@@ -334,13 +312,8 @@ void build_model(Context& ctx, ModelTables& t, const float* xyz, const float* nx
   {
     DevBuf words;
     words.reserve(t.P * sizeof(unsigned long long));
-    if (ctx.entry_order_angle)
-      order_words_angle_kernel<<<grid_for(t.P, 256), 256, 0, st>>>(
-          t.keys.as<uint32_t>(), t.pairs.as<uint32_t>(), t.P, t.n, t.pts.as<float4>(), t.frame_r1.as<float4>(),
-          t.frame_r2.as<float4>(), words.as<unsigned long long>());
-    else
-      order_words_kernel<<<grid_for(t.P, 256), 256, 0, st>>>(t.keys.as<uint32_t>(), t.pairs.as<uint32_t>(),
-                                                              t.P, t.n, words.as<unsigned long long>());
+    order_words_kernel<<<grid_for(t.P, 256), 256, 0, st>>>(t.keys.as<uint32_t>(), t.pairs.as<uint32_t>(),
+                                                            t.P, t.n, words.as<unsigned long long>());
     PPF_CUDA(cudaMemcpyAsync(t.epairs.ptr, t.pairs.ptr, t.P * 4, cudaMemcpyDeviceToDevice, st));
     PPF_CUDA(cudaGetLastError());
     size_t l1 = ctx.sort64.launches();

@@ -362,12 +362,23 @@ __device__ __forceinline__ void vote_item(const VoteArgs& a, uint32_t slot_of_it
           // kUnroll entries per lane per pass, branch-free: the fast cell of
           // every vote is counted, and the rare votes near a bin edge are
           // moved afterwards.  The last pass is masked to the segment's end.
+          // The loads of the next pass are issued before this pass's
+          // atomics, so the L2 latency of the entries overlaps the counting.
           const uint32_t nfull = n_here / (32 * kUnroll);
+          uint32_t nx[kUnroll];
+          if (nfull) {
+#pragma unroll
+            for (int u = 0; u < kUnroll; ++u) nx[u] = __ldg(ep + 32 * u);
+          }
           for (uint32_t it = 0; it < nfull; ++it, ep += 32 * kUnroll) {
             uint32_t c[kUnroll];
             bool amb = false;
 #pragma unroll
-            for (int u = 0; u < kUnroll; ++u) c[u] = __ldg(ep + 32 * u);
+            for (int u = 0; u < kUnroll; ++u) c[u] = nx[u];
+            if (it + 1 < nfull) {
+#pragma unroll
+              for (int u = 0; u < kUnroll; ++u) nx[u] = __ldg(ep + 32 * kUnroll + 32 * u);
+            }
 #pragma unroll
             for (int u = 0; u < kUnroll; ++u) {
               const uint32_t y = bsh - (c[u] << kShift);

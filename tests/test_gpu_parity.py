@@ -419,25 +419,3 @@ def test_cpp_facade_matches_python_api(pkg, ctx, tmp_path):
         got = np.array([int(h, 16) for h in lines[tag]], np.uint32).view(np.float32).reshape(4, 4)
         assert _same(got, want), tag
 
-
-def test_entry_orders_give_identical_results(pkg, ctx, monkeypatch):
-    """Vote entries of a (key, m_r) ordered by angle (PPF_B200_ENTRY_ORDER=
-    angle) or by a hash of the pair count the same votes: identical cells,
-    kept votes, scores and pose, on a model of three chunks."""
-    spec = pkg.synthetic.config_plain(seed=171, n_model=3500, n_plane=2500, n_box=800)
-    m, s, d = spec.models[0], spec.scene, spec.d_dists[0]
-    monkeypatch.setenv("PPF_B200_ENTRY_ORDER", "angle")
-    actx = pkg.Context(0)
-    a = pkg.Model(m, d, 0.3, context=ctx)
-    b = pkg.Model(m, d, 0.3, context=actx)
-    assert a.num_chunks == b.num_chunks == 3
-    sa, sb = pkg.Scene(s, d, 5, context=ctx), pkg.Scene(s, d, 5, context=actx)
-    pa, pb = a.ppf_lookup(sa).copy(), b.ppf_lookup(sb).copy()
-    assert _same(pa, pb)
-    for x, y in zip(a.get_votes(), b.get_votes()):
-        assert np.array_equal(x, y)
-    for x, y in zip(a.get_cluster_state(), b.get_cluster_state()):
-        assert _same(x, y)
-    ca, ka = a.all_votes(sa)
-    cb, kb = b.all_votes(sb)
-    assert np.array_equal(ca, cb) and np.array_equal(ka, kb)
