@@ -25,7 +25,11 @@
 namespace ppf {
 namespace {
 
-constexpr uint32_t kSeg = 1024;   // entries per segment
+// Entries per segment.  A warp streams a segment in passes of 256 entries
+// and pays the L2 latency of its first loads and the segment search once per
+// segment: 1024/2048/4096/8192 measured 57.8/53.2/51.5/51.6 ms on the bench's
+// first model (ref_point_df 50), and the bench's vote launch 1890/1762/1716/1716 ms.
+constexpr uint32_t kSeg = 4096;
 constexpr int kUnroll = 8;        // independent entry loads per lane
 constexpr uint32_t kNoRun = 0xffffffffu;
 constexpr uint32_t kExactOnly = 1u << 31;  // scene angle flag: every vote of the pair takes the exact path
@@ -362,23 +366,12 @@ __device__ __forceinline__ void vote_item(const VoteArgs& a, uint32_t slot_of_it
           // kUnroll entries per lane per pass, branch-free: the fast cell of
           // every vote is counted, and the rare votes near a bin edge are
           // moved afterwards.  The last pass is masked to the segment's end.
-          // The loads of the next pass are issued before this pass's
-          // atomics, so the L2 latency of the entries overlaps the counting.
           const uint32_t nfull = n_here / (32 * kUnroll);
-          uint32_t nx[kUnroll];
-          if (nfull) {
-#pragma unroll
-            for (int u = 0; u < kUnroll; ++u) nx[u] = __ldg(ep + 32 * u);
-          }
           for (uint32_t it = 0; it < nfull; ++it, ep += 32 * kUnroll) {
             uint32_t c[kUnroll];
             bool amb = false;
 #pragma unroll
-            for (int u = 0; u < kUnroll; ++u) c[u] = nx[u];
-            if (it + 1 < nfull) {
-#pragma unroll
-              for (int u = 0; u < kUnroll; ++u) nx[u] = __ldg(ep + 32 * kUnroll + 32 * u);
-            }
+            for (int u = 0; u < kUnroll; ++u) c[u] = __ldg(ep + 32 * u);
 #pragma unroll
             for (int u = 0; u < kUnroll; ++u) {
               const uint32_t y = bsh - (c[u] << kShift);
