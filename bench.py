@@ -674,6 +674,7 @@ def main():
                      "alg_bytes_per_launch": alg_bytes / args.steps,
                      "vote_ms_per_launch": vote_ms / args.steps},
         "gpu_launches": int(launches),
+        "vote_segments_tuned": [int(s["vote_segment"]) for s in stats[0]],
         "recall": recall,
         "clocks": clk.summary(),
     }

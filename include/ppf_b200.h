@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define PPF_B200_ABI_VERSION 2
+#define PPF_B200_ABI_VERSION 3
 
 typedef enum ppf_status {
   PPF_OK = 0,
@@ -59,6 +59,10 @@ typedef struct ppf_stats {
   uint32_t n_redo_items;     /* vote items emitted again after the candidate buffer grew */
   uint32_t cluster_path;     /* clustering that ran: 0 none, 1 ordered sums per cell tile,
                                 2 per-pose neighbour lists, 3 split exact sums, 4 greedy */
+  uint32_t vote_segment;     /* entries per warp segment of the vote pass: chosen per model
+                                by timing sample vote launches on the model's first lookup
+                                (the same choice for every later lookup of a model with the
+                                same points count, d_dist and threshold on this context) */
 } ppf_stats;
 
 /* Error text of the last failing call on this thread ("" if none). */

@@ -39,6 +39,7 @@ class ppf_stats(C.Structure):
         ("gpu_launches", C.c_uint32),
         ("n_redo_items", C.c_uint32),
         ("cluster_path", C.c_uint32),
+        ("vote_segment", C.c_uint32),
     ]
 
     def as_dict(self):

@@ -112,6 +112,8 @@ LookupOut finish_lookup(Context& ctx, Model& m, LookupState& st, const SceneData
   out.stats.n_exact_bins = vr.n_exact;
   out.stats.max_vote_count = vr.max_count;
   out.stats.vote_ms = vr.vote_ms;
+  const uint32_t shift = m.seg_shift.load(std::memory_order_relaxed);
+  out.stats.vote_segment = 1u << (shift ? shift : kSegShiftDefault);
   out.stats.n_redo_items = vr.n_redo;
   if (vr.max_count == 0) {
     out.status = PPF_ERR_NO_VOTES;
@@ -160,6 +162,7 @@ LookupOut finish_lookup(Context& ctx, Model& m, LookupState& st, const SceneData
 LookupOut lookup(Model& m, const SceneData& s) {
   Context& ctx = *m.ctx;
   const size_t launches0 = ctx.launches;
+  tune_vote_segments(ctx, m, s, model_signature(m));
   PPF_CUDA(cudaEventRecord(ctx.ev[2], ctx.stream));
   VoteResult vr = run_votes(ctx, m, s, false, -1.f);
   return finish_lookup(ctx, m, m.last, s, vr, ctx.cand_codes.as<unsigned long long>(),
@@ -174,6 +177,7 @@ std::vector<LookupOut> lookup_batch(Context& ctx, const std::vector<Model*>& mod
                                     const size_t* caps) {
   const size_t n = models.size();
   const size_t launches0 = ctx.launches;
+  for (size_t i = 0; i < n; ++i) tune_vote_segments(ctx, *models[i], *scenes[i], model_signature(*models[i]));
   PPF_CUDA(cudaEventRecord(ctx.ev[2], ctx.stream));
   std::vector<BatchVote> reqs(n);
   constexpr size_t kBudgetCells = size_t(1) << 28;  // 3 GB of candidate cells over the batch
@@ -237,6 +241,13 @@ void init_context(Context& c, int device) {
   c.vote_smem_limit = optin - 2048;  // static shared memory of the vote kernel
   if (const char* e = std::getenv("PPF_B200_CHECKS")) c.checks = e[0] == '1';
   if (const char* e = std::getenv("PPF_B200_CLUSTER_SPLIT")) c.cluster_split = e[0] != '0';
+  if (const char* e = std::getenv("PPF_B200_TUNE")) c.tune = e[0] != '0';
+  if (const char* e = std::getenv("PPF_B200_VOTE_SEGMENT")) {
+    // a power of two from 256 to 65536 entries
+    const long long v = std::atoll(e);
+    for (uint32_t k = 8; k <= 16; ++k)
+      if (v == (1ll << k)) c.forced_seg_shift = k;
+  }
   // test hooks: the n-th device allocation from now fails; the next 32-bit
   // radix sort on this context has one tile withhold its look-back status,
   // so that the tiles waiting on it give up after a short bounded spin

@@ -46,6 +46,12 @@ struct Context {
   // (points, d_dist, threshold) emitted; sizes the next batch's buffers when
   // the same model is built again
   std::unordered_map<uint64_t, size_t> cand_hints;
+  // vote segment length chosen by the tuner per model signature
+  // (tune_vote_segments); PPF_B200_TUNE=0 keeps the default
+  std::unordered_map<uint64_t, uint32_t> seg_tuned;
+  bool tune = true;
+  uint32_t forced_seg_shift = 0;  // PPF_B200_VOTE_SEGMENT=<2^k>: every model uses it
+  DevBuf tune_counters;
   size_t cand_cap = size_t(1) << 24;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   int vote_smem_limit = 0;  // max dynamic shared memory per vote block
@@ -120,6 +126,10 @@ struct Model {
   float vote_count_threshold = 0.4f;
   bool cpu_clustering = false, use_l1_norm = false, use_averaged_clusters = false;
   size_t cand_hint = 0;  // candidate cells of the last vote pass (sizes batch buffers)
+  // log2 of the vote pass's segment length (entries a warp streams per
+  // segment); 0 until the tuner has chosen it (the default is used)
+  // (atomic: the workers of a server may tune one library model at once)
+  std::atomic<uint32_t> seg_shift{0};
   LookupState last;
 };
 
@@ -169,6 +179,14 @@ void pair_vote_counts(Context& ctx, const Model& m, const SceneData& s, uint64_t
 void vote_cells_noalloc(Context& ctx, const Model& m, const float* xyz, const float* nxyz,
                         uint64_t n, uint32_t ref_df, float vote_floor, uint64_t* codes,
                         uint32_t* counts, uint64_t capacity, uint64_t* n_out, uint32_t* max_out);
+
+// Default log2 segment length of the vote pass and the tuner's candidates.
+constexpr uint32_t kSegShiftDefault = 12;
+// Chooses the vote pass's segment length for model m on its first lookup
+// (per model signature, cached in the context): short vote launches over a
+// sample of the work items of (m, s), counting only, one per candidate.
+void tune_vote_segments(Context& ctx, Model& m, const SceneData& s, uint64_t signature);
+uint64_t model_signature(const Model& m);
 
 // ---- poses and clustering (pose.cu)
 // Filters the candidates to the kept votes and orders them (count desc,

@@ -7,7 +7,7 @@
 // counter.  For its s_r it walks all scene points in tiles of 1024: each
 // thread computes one pair feature, its FNV key, and looks the key up in the
 // model's key -> run table.  Every matched pair's sub-run (the run entries
-// whose m_r falls in this chunk) is cut into segments of at most kSeg entries;
+// whose m_r falls in this chunk) is cut into segments of at most 2^seg_shift entries;
 // warps take segments from a shared counter and stream their entries with
 // consecutive lanes on consecutive entries, counting each vote into a
 // shared-memory accumulator of 32-bit (m_r, alpha bin) counters.  When an
@@ -25,11 +25,14 @@
 namespace ppf {
 namespace {
 
-// Entries per segment.  A warp streams a segment in passes of 256 entries
-// and pays the L2 latency of its first loads and the segment search once per
-// segment: 1024/2048/4096/8192 measured 57.8/53.2/51.5/51.6 ms on the bench's
-// first model (ref_point_df 50), and the bench's vote launch 1890/1762/1716/1716 ms.
-constexpr uint32_t kSeg = 4096;
+// Entries per segment: 1 << VoteArgs::seg_shift.  A warp streams a segment
+// in passes of 256 entries and pays the L2 latency of its first loads and the
+// segment search once per segment; longer segments leave more warps idle at
+// the end of a tile.  Fixed lengths of 1024/2048/4096/8192 measured
+// 57.8/53.2/51.5/51.6 ms on the bench's first model (ref_point_df 50) and
+// 92.1/83.8/79.8/78.3 ms on its fourth: the best length depends on the model,
+// so tune_vote_segments chooses it per model among kSegShifts.
+constexpr uint32_t kSegShifts[] = {11, 12, 13};
 constexpr int kUnroll = 8;        // independent entry loads per lane
 constexpr uint32_t kNoRun = 0xffffffffu;
 constexpr uint32_t kExactOnly = 1u << 31;  // scene angle flag: every vote of the pair takes the exact path
@@ -48,6 +51,7 @@ struct VoteArgs {
   const float4* m_r2;
   const float4* m_pts;
   uint32_t n_m, chunk, n_chunks;
+  uint32_t seg_shift;  // log2 of the segment length
   // scene
   const float4* s_pts;
   const float4* s_nrm;
@@ -227,6 +231,7 @@ __device__ __forceinline__ void vote_item(const VoteArgs& a, uint32_t slot_of_it
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t cells = a.chunk * kBins;
+  const uint32_t seg_len = 1u << a.seg_shift;
   {
     const uint32_t item = a.item_list ? a.item_list[slot_of_item] : slot_of_item;
     const uint32_t c = item % a.n_chunks;
@@ -273,7 +278,7 @@ __device__ __forceinline__ void vote_item(const VoteArgs& a, uint32_t slot_of_it
         }
       }
       uint32_t n_seg_total;
-      const uint32_t seg0 = block_excl_scan((len + kSeg - 1) / kSeg, sh.scan_seg, n_seg_total);
+      const uint32_t seg0 = block_excl_scan((len + seg_len - 1) >> a.seg_shift, sh.scan_seg, n_seg_total);
       q_lo[tid] = lo;
       q_len[tid] = len;
       q_beta[tid] = beta;
@@ -286,7 +291,7 @@ __device__ __forceinline__ void vote_item(const VoteArgs& a, uint32_t slot_of_it
       }
       block_sync();
       if (kCheck) {
-        const uint32_t want = q_seg[tid] + (q_len[tid] + kSeg - 1) / kSeg;
+        const uint32_t want = q_seg[tid] + ((q_len[tid] + seg_len - 1) >> a.seg_shift);
         if (q_seg[tid] != seg0 || q_seg[tid + 1] != want)
           in_range<kCheck>(a, 11, ((unsigned long long)tid << 32) | q_seg[tid + 1], want);
       }
@@ -301,8 +306,8 @@ __device__ __forceinline__ void vote_item(const VoteArgs& a, uint32_t slot_of_it
         const uint32_t blk = 31u - __clz(__ballot_sync(0xffffffffu, sh.seg_blk[lane] <= s));
         const uint32_t plo = 32u * blk + 31u - __clz(__ballot_sync(0xffffffffu, q_seg[32 * blk + lane] <= s));
         const uint32_t p = plo;
-        const uint32_t start = q_lo[p] + (s - q_seg[p]) * kSeg;
-        uint32_t end = min(q_lo[p] + q_len[p], start + kSeg);
+        const uint32_t start = q_lo[p] + ((s - q_seg[p]) << a.seg_shift);
+        uint32_t end = min(q_lo[p] + q_len[p], start + seg_len);
         // Always-on guard (one compare per segment of up to 1024 votes): a
         // segment outside its sub-run or the entry array is recorded, raises
         // kFlagBadIndex and is skipped, so the lookup fails instead of the
@@ -589,6 +594,8 @@ VoteArgs make_args(const Model& m, const SceneData& s) {
   a.n_m = t.n;
   a.chunk = t.chunk;
   a.n_chunks = t.n_chunks;
+  const uint32_t shift = m.seg_shift.load(std::memory_order_relaxed);
+  a.seg_shift = shift ? shift : kSegShiftDefault;
   a.s_pts = s.pts.as<float4>();
   a.s_nrm = s.nrm.as<float4>();
   a.n_s = s.n;
@@ -851,6 +858,84 @@ void run_votes_batch(Context& ctx, std::vector<BatchVote>& reqs) {
     // the batch's device time, split by work items
     r.vote_ms = total ? ms * (float)(item_off[i + 1] - item_off[i]) / (float)total : 0.f;
   }
+}
+
+void tune_vote_segments(Context& ctx, Model& m, const SceneData& s, uint64_t signature) {
+  if (m.seg_shift) return;
+  if (ctx.forced_seg_shift) {
+    m.seg_shift = ctx.forced_seg_shift;
+    return;
+  }
+  auto it = ctx.seg_tuned.find(signature);
+  if (it != ctx.seg_tuned.end()) {
+    m.seg_shift = it->second;
+    return;
+  }
+  if (!ctx.tune || s.n < 2) {
+    m.seg_shift = kSegShiftDefault;
+    return;
+  }
+  cudaStream_t stream = ctx.stream;
+  VoteArgs a = make_args(m, s);
+  const uint32_t n_items = a.n_ref * a.n_chunks;
+  // about two items per SM: the first items of the pass's scrambled order of
+  // scene reference points, for every chunk of the model
+  const uint32_t sample = std::min<uint32_t>(n_items, 2u * (uint32_t)sm_count());
+  // The sample launches count and emit nothing: no cell exceeds an infinite
+  // floor.  Their counters live in a buffer of their own.
+  ctx.tune_counters.reserve(64 + 32 + 80);
+  uint32_t* cnt = ctx.tune_counters.as<uint32_t>();
+  a.emit_all = 0;
+  a.floor = INFINITY;
+  a.work_counter = cnt + 0;
+  a.global_max = cnt + 1;
+  a.n_cand = cnt + 2;
+  a.n_redo = cnt + 3;
+  a.stats = reinterpret_cast<unsigned long long*>(cnt + 4);
+  a.n_needed = reinterpret_cast<unsigned long long*>(cnt + 10);
+  a.flags = cnt + 16;
+  a.bad = reinterpret_cast<unsigned long long*>(cnt + 24);
+  a.cand_code = nullptr;
+  a.cand_count = nullptr;
+  a.cand_cap = 0;
+  a.redo_items = nullptr;
+  a.n_items_total = 0;
+  a.item_list = nullptr;
+  a.n_items = sample;
+  const size_t smem = kVoteQueueBytes + vote_acc_words(a.chunk) * 4;
+  PPF_REQUIRE((int)smem <= ctx.vote_smem_limit, PPF_ERR_INTERNAL, "vote accumulator too large");
+  auto kernel = vote_kernel<false>;
+  PPF_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  constexpr int kCands = sizeof(kSegShifts) / sizeof(kSegShifts[0]);
+  float best_ms[kCands];
+  for (int c = 0; c < kCands; ++c) best_ms[c] = INFINITY;
+  // two rounds over the candidates, the faster of each candidate's two times
+  for (int round = 0; round < 2; ++round)
+    for (int c = 0; c < kCands; ++c) {
+      a.seg_shift = kSegShifts[c];
+      PPF_CUDA(cudaMemsetAsync(cnt, 0, 64 + 32 + 80, stream));
+      PPF_CUDA(cudaEventRecord(ctx.ev[0], stream));
+      kernel<<<std::min<uint32_t>(sample, (uint32_t)sm_count()), kVoteThreads, smem, stream>>>(a);
+      PPF_CUDA(cudaGetLastError());
+      ctx.launches++;
+      PPF_CUDA(cudaEventRecord(ctx.ev[1], stream));
+      PPF_CUDA(cudaEventSynchronize(ctx.ev[1]));
+      float ms = 0;
+      PPF_CUDA(cudaEventElapsedTime(&ms, ctx.ev[0], ctx.ev[1]));
+      best_ms[c] = std::min(best_ms[c], ms);
+    }
+  uint32_t flags = 0;
+  PPF_CUDA(cudaMemcpyAsync(&flags, cnt + 16, sizeof(flags), cudaMemcpyDeviceToHost, stream));
+  PPF_CUDA(cudaStreamSynchronize(stream));
+  PPF_REQUIRE(!(flags & kFlagBadIndex), PPF_ERR_INTERNAL, "vote kernel index out of range while tuning");
+  // the default stays unless another length is at least 2% faster
+  int pick = -1;
+  for (int c = 0; c < kCands; ++c)
+    if (kSegShifts[c] == kSegShiftDefault) pick = c;
+  for (int c = 0; c < kCands; ++c)
+    if (best_ms[c] < 0.98f * best_ms[pick]) pick = c;
+  m.seg_shift = kSegShifts[pick];
+  ctx.seg_tuned[signature] = m.seg_shift;
 }
 
 void pair_vote_counts(Context& ctx, const Model& m, const SceneData& s, uint64_t* out_dev) {

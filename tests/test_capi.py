@@ -24,7 +24,7 @@ def test_library_exports_every_header_symbol(pkg):
 
 def test_abi_version_and_error_text(pkg):
     lib = pkg.load()
-    assert lib.ppf_abi_version() == 2
+    assert lib.ppf_abi_version() == 3
     assert lib.ppf_last_error() is not None
 
 

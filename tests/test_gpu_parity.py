@@ -419,3 +419,27 @@ def test_cpp_facade_matches_python_api(pkg, ctx, tmp_path):
         got = np.array([int(h, 16) for h in lines[tag]], np.uint32).view(np.float32).reshape(4, 4)
         assert _same(got, want), tag
 
+
+
+def test_vote_segment_lengths_give_identical_results(pkg, ctx, monkeypatch):
+    """The vote pass's segment length (chosen per model by the tuner, or fixed
+    with PPF_B200_VOTE_SEGMENT) changes only how warps share the work: every
+    vote cell, the kept votes, scores and pose are the same for all lengths."""
+    spec = pkg.synthetic.config_plain(seed=172, n_model=2500, n_plane=3000, n_box=1000)
+    m, s, d = spec.models[0], spec.scene, spec.d_dists[0]
+    tuned = pkg.Model(m, d, 0.3, context=ctx)
+    scene = pkg.Scene(s, d, 5, context=ctx)
+    pose = tuned.ppf_lookup(scene).copy()
+    assert tuned.stats["vote_segment"] in (2048, 4096, 8192)
+    votes, state = tuned.get_votes(), tuned.get_cluster_state()
+    cells = tuned.all_votes(scene)
+    for seg in (256, 1024, 8192):
+        monkeypatch.setenv("PPF_B200_VOTE_SEGMENT", str(seg))
+        c = pkg.Context(0)
+        other = pkg.Model(m, d, 0.3, context=c)
+        sc = pkg.Scene(s, d, 5, context=c)
+        assert _same(other.ppf_lookup(sc), pose)
+        assert other.stats["vote_segment"] == seg
+        assert all(np.array_equal(x, y) for x, y in zip(other.get_votes(), votes))
+        assert all(_same(x, y) for x, y in zip(other.get_cluster_state(), state))
+        assert all(np.array_equal(x, y) for x, y in zip(other.all_votes(sc), cells))
