@@ -25,6 +25,7 @@ Context::~Context() {
   batch_counters.release();
   batch_redo.release();
   redo_items.release();
+  tune_counters.release();
   sort32.release();
   sort64.release();
   if (stream) cudaStreamSynchronize(stream);

@@ -31,6 +31,8 @@ inline size_t vote_acc_words(uint32_t chunk) { return ((size_t)chunk * kBins + 3
 // Angle quantum on the host (include/kernel.h:16 evaluated in float).
 #define PPF_D_ANGLE_HOST ((2.0f * 3.141592654f) / float(30))
 
+// Every DevBuf member must be released in ~Context (capi.cu) before the
+// stream its blocks are freed on is destroyed.
 struct Context {
   int device = 0;
   cudaStream_t stream = nullptr;
