@@ -332,15 +332,17 @@ def run_serve(args):
     reqs = [(sc, sorted({i.model_index for i in inst})) for sc, inst in scenes]
     n_reg = sum(len(ids) for _, ids in reqs)
 
-    def plain_all():
+    def plain_all(subset=None):
         out = []
-        for sc, ids in reqs:
+        for sc, ids in (reqs if subset is None else subset):
             p = pkg.ppf_registration([sc], [models[j] for j in ids], [d_dists[j] for j in ids], REF_DF, THR,
                                      context=ctx)
             out.append(np.asarray(p[0]))
         return out
 
-    plain_all()  # warm-up (pool, hints)
+    # warm-up (pool, tuner, candidate hints): every request for the small
+    # preset, the first one for the library configs
+    plain_all(None if args.serve_preset == "small" else reqs[:1])
     ctx.synchronize()
     t0 = time.perf_counter()
     plain = plain_all()
@@ -349,15 +351,15 @@ def run_serve(args):
 
     lib = [pkg.Model(m, d, THR, context=ctx) for m, d in zip(models, d_dists)]
 
-    def batched_all():
+    def batched_all(subset=None):
         ms, ss = [], []
-        for sc, ids in reqs:
+        for sc, ids in (reqs if subset is None else subset):
             for j in ids:
                 ms.append(lib[j])
                 ss.append(pkg.Scene(sc, d_dists[j], REF_DF, context=ctx))
         return pkg.lookup_batch(ms, ss, context=ctx, raise_on_no_votes=False)
 
-    batched_all()
+    batched_all(None if args.serve_preset == "small" else reqs[:2])
     ctx.synchronize()
     t0 = time.perf_counter()
     batched_all()
