@@ -561,6 +561,8 @@ def main():
         return pkg.ppf_registration([scene], models, spec.d_dists, REF_DF, THR, False, False, args.avg,
                                     local, None, context=ctx, return_stats=True)
 
+    # vote chunks of each model (queried once, outside the timed region)
+    chunks = [pkg.Model(m, d, THR, context=ctx).num_chunks for m, d in zip(models_d, spec.d_dists)]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
     def flush_l2():
@@ -604,7 +606,9 @@ def main():
         sys.stderr.write(f"bench: poses of models {changed} changed between warm-up and timed steps\n")
         sys.exit(3)
     n_ref = (len(spec.scene) + REF_DF - 1) // REF_DF
-    pairs = n_ref * len(spec.scene) * len(spec.models) * args.steps
+    # every (scene reference point, chunk) work item walks the whole scene, so
+    # a model of C chunks evaluates each scene pair C times
+    pairs = n_ref * len(spec.scene) * sum(chunks) * args.steps
     ms_max = reduce_max(dist, ms, dev)
     regs = world * len(spec.models) * args.steps
     value = regs / (ms_max / 1000.0)
@@ -674,6 +678,8 @@ def main():
                                      "algorithmic bytes reach DRAM), and the kernel is limited by shared-memory "
                                      "atomic wavefronts (l1tex 75% of peak on the profile case)",
                      "alg_bytes_per_launch": alg_bytes / args.steps,
+                     "alg_bytes_rule": "4 B per vote + 32 B per scene pair evaluated (pairs x vote chunks of the model)",
+                     "vote_chunks": chunks,
                      "vote_ms_per_launch": vote_ms / args.steps},
         "gpu_launches": int(launches),
         "vote_segments_tuned": [int(s["vote_segment"]) for s in stats[0]],
