@@ -2,6 +2,7 @@
 // spatial-hash pose clustering and the best pose
 // (src/cuda/model.cu:155-244,293-295, src/cuda/ppf.cu:78-93).
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 
 #include "engine.h"
@@ -218,16 +219,36 @@ __global__ void cluster_kernel(ClusterArgs a) {
 
 constexpr int kClusterTile = 256;
 
+// Also folds the largest squared norm of a finite quaternion into *max_qq
+// (float bits; non-negative floats order as their bits).
 __global__ void gather_sorted_kernel(const uint32_t* __restrict__ map, size_t U,
                                      const float* __restrict__ quats, const float* __restrict__ trans0,
                                      const float* __restrict__ weighted, float4* __restrict__ qs,
-                                     float4* __restrict__ tws) {
+                                     float4* __restrict__ tws, uint32_t* __restrict__ max_qq) {
+  float m = 0.f;
   for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < U;
        p += (size_t)gridDim.x * blockDim.x) {
     uint32_t o = map[p];
-    qs[p] = make_float4(quats[4 * o], quats[4 * o + 1], quats[4 * o + 2], quats[4 * o + 3]);
+    const float4 q = make_float4(quats[4 * o], quats[4 * o + 1], quats[4 * o + 2], quats[4 * o + 3]);
+    qs[p] = q;
     tws[p] = make_float4(trans0[3 * o], trans0[3 * o + 1], trans0[3 * o + 2], weighted[o]);
+    const float qq = q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w;
+    if (isfinite(qq)) m = fmaxf(m, qq);
   }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(max_qq, __float_as_uint(m));
+}
+
+// Quaternion half-width of the box filters.  The reference's rotation test
+// passes only if |8 (1 - q.s)| < rot_sq, so q.s > 1 - rot_sq / 8, and then
+// |q - s|^2 = |q|^2 + |s|^2 - 2 q.s < 2 R^2 - 2 + rot_sq / 4 for quaternions
+// of norm at most R: every component of q - s is within that root (0.2095
+// for unit quaternions).  The small additions cover float rounding.
+float quat_margin(float max_qq) {
+  const double rot_sq = (double)(2 * PPF_D_ANGLE_HOST) * (double)(2 * PPF_D_ANGLE_HOST);
+  const double r2 = std::max(0.0, 2.0 * (double)max_qq - 2.0);
+  return (float)(std::sqrt(r2 + rot_sq / 4.0 + 1e-5) + 1e-5);
 }
 
 // Whether two different int3 cells share one cell key (then the per-pose
@@ -304,6 +325,7 @@ struct TiledArgs {
   const float4* qs;
   const float4* tws;
   float d_dist;
+  float qmargin;  // quaternion half-width of the box filter (quat_margin)
   int use_l1, use_avg;
   float* scores;
   float* trans;
@@ -325,8 +347,8 @@ __device__ __forceinline__ float warp_max(float v) {
 // bucket, and streams the poses of the cell's neighbour cells through shared
 // memory in the reference's order (neighbour b = 0..26, then position).  Each
 // warp first marks, with one ballot per 32 sources, the sources inside a box
-// around its targets: quaternion components within 0.25 of some target's
-// (the rotation test implies a quaternion distance below 2*pi/30 < 0.21) and,
+// around its targets: quaternion components within quat_margin of some
+// target's (about 0.21: the rotation test bounds the quaternion distance) and,
 // in L2 mode, translation components within 1.0001 d_dist.  It then runs the
 // reference's tests on the marked sources only, in ascending order, so every
 // target adds the same weights in the same order as the reference.
@@ -334,7 +356,7 @@ __global__ void __launch_bounds__(kClusterTile) cluster_tiled_kernel(TiledArgs a
   __shared__ float4 sq[kClusterTile], stw[kClusterTile];
   const float rot_sq = PPF_ROT_THRESH * PPF_ROT_THRESH;
   const int lane = threadIdx.x & 31;
-  constexpr float kQuatMargin = 0.25f;
+  const float kQuatMargin = a.qmargin;
   const float t_margin = a.use_l1 ? INFINITY : a.d_dist * 1.0001f + 1e-6f;
   for (uint32_t item = blockIdx.x; item < a.n_items; item += gridDim.x) {
     size_t lo = 0, hi = a.Kc;  // run r with item_off[r] <= item < item_off[r + 1]
@@ -491,7 +513,7 @@ constexpr int kSplitBlock = 256;
 __global__ void __launch_bounds__(kSplitBlock) cluster_split_kernel(TiledArgs a) {
   const float rot_sq = PPF_ROT_THRESH * PPF_ROT_THRESH;
   const int lane = threadIdx.x & 31;
-  constexpr float kQuatMargin = 0.25f;  // as cluster_tiled_kernel
+  const float kQuatMargin = a.qmargin;  // as cluster_tiled_kernel
   const float t_margin = a.use_l1 ? INFINITY : a.d_dist * 1.0001f + 1e-6f;
   const uint32_t n_warps = gridDim.x * (kSplitBlock / 32);
   for (uint32_t item = blockIdx.x * (kSplitBlock / 32) + (threadIdx.x >> 5); item < a.n_items;
@@ -776,10 +798,11 @@ size_t cluster_poses_gpu(Context& ctx, const Model& m, LookupState& st, float* b
   const bool may_split = ctx.cluster_split && !m.use_averaged_clusters;
   uint32_t* item_off32 = may_split ? grow<uint32_t>(st.item_off32, Kc + 1) : nullptr;
   // counters: [0] mixed cells, [1] tiles, [2] split items, [3] non-integer
-  // weight, [4..5] sum of |weight|
-  PPF_CUDA(cudaMemsetAsync(ctx.counters.ptr, 0, 24, stream));
+  // weight, [4..5] sum of |weight|, [6] largest squared quaternion norm
+  PPF_CUDA(cudaMemsetAsync(ctx.counters.ptr, 0, 28, stream));
   uint32_t* mixed = ctx.counters.as<uint32_t>();
-  gather_sorted_kernel<<<grid_for(U, 256), 256, 0, stream>>>(map, U, a.quats, a.trans0, a.weighted, qs, tws);
+  gather_sorted_kernel<<<grid_for(U, 256), 256, 0, stream>>>(map, U, a.quats, a.trans0, a.weighted, qs, tws,
+                                                              mixed + 6);
   mixed_cells_kernel<<<grid_for(U, 256), 256, 0, stream>>>(ck, map, st.cells3.as<int4>(), U, mixed);
   run_adjacency_kernel<<<grid_for(Kc, 128), 128, 0, stream>>>(fi, ct, Kc, map, st.cells3.as<int4>(), uq,
                                                               adjrun, item_off, item_off32);
@@ -791,9 +814,12 @@ size_t cluster_poses_gpu(Context& ctx, const Model& m, LookupState& st, float* b
                                                               reinterpret_cast<unsigned long long*>(mixed + 4));
     ctx.launches += 2;
   }
-  uint32_t hc[6];
+  uint32_t hc[7];
   PPF_CUDA(cudaMemcpyAsync(hc, mixed, sizeof(hc), cudaMemcpyDeviceToHost, stream));
   PPF_CUDA(cudaStreamSynchronize(stream));
+  float max_qq;
+  std::memcpy(&max_qq, hc + 6, sizeof(max_qq));
+  const float qmargin = quat_margin(max_qq);
   const unsigned long long abs_sum = hc[4] | ((unsigned long long)hc[5] << 32);
   const bool split = may_split && !hc[0] && !hc[3] && abs_sum < (1ull << 24) - 1;
   st.cluster_path = split ? 3 : hc[0] ? 2 : 1;
@@ -818,6 +844,7 @@ size_t cluster_poses_gpu(Context& ctx, const Model& m, LookupState& st, float* b
     ta.qs = qs;
     ta.tws = tws;
     ta.d_dist = m.t.d_dist;
+    ta.qmargin = qmargin;
     ta.use_l1 = m.use_l1_norm;
     ta.use_avg = 0;
     ta.scores = a.scores;
@@ -849,6 +876,7 @@ size_t cluster_poses_gpu(Context& ctx, const Model& m, LookupState& st, float* b
     ta.qs = qs;
     ta.tws = tws;
     ta.d_dist = m.t.d_dist;
+    ta.qmargin = qmargin;
     ta.use_l1 = m.use_l1_norm;
     ta.use_avg = m.use_averaged_clusters;
     ta.scores = a.scores;
