@@ -118,6 +118,7 @@ struct LookupState {
   DevBuf tmp64, tmp32a, tmp32b, tmp32c, perm;
   DevBuf tperm;       // clustering target order (cell, rotation bucket)
   DevBuf best;        // float[16] pose + int idx
+  DevBuf argmax_v, argmax_i;  // per-block partial maxima of the scores
   uint32_t cluster_path = 0;  // ppf_stats::cluster_path of the last clustering
   std::vector<float> cpu_poses;
 };

@@ -580,31 +580,23 @@ __global__ void __launch_bounds__(kSplitBlock) cluster_split_kernel(TiledArgs a)
   }
 }
 
-// First index of the largest score (thrust::max_element semantics), then the
-// pose assembly of ppf.cu:78-93 into best[0..15]; best[16] = score and
-// best[18..19] = index (uint64).
-__global__ void argmax_pose_kernel(const float* __restrict__ scores, size_t U,
-                                   const float* __restrict__ transforms,
-                                   const float* __restrict__ trans, float* __restrict__ best) {
+// First index of the largest score (thrust::max_element semantics: NaN never
+// wins, the first of equal maxima does), in two steps: each block reduces a
+// strided share of the scores to (value, index) pairs, then one block
+// reduces those and assembles the pose of ppf.cu:78-93 into best[0..15];
+// best[16] = score and best[18..19] = index (uint64).
+__device__ __forceinline__ void argmax_take(float v, unsigned long long i, float& bv, unsigned long long& bi) {
+  if (v > bv || (v == bv && i < bi)) {
+    bv = v;
+    bi = i;
+  }
+}
+
+__device__ __forceinline__ void block_argmax(float& bv, unsigned long long& bi) {
   __shared__ float s_v[32];
   __shared__ unsigned long long s_i[32];
-  float bv = -INFINITY;
-  unsigned long long bi = ~0ull;
-  for (size_t i = threadIdx.x; i < U; i += blockDim.x) {
-    float v = scores[i];
-    if (v > bv || (v == bv && i < bi)) {
-      bv = v;
-      bi = i;
-    }
-  }
-  for (int o = 16; o; o >>= 1) {
-    float ov = __shfl_xor_sync(0xffffffffu, bv, o);
-    unsigned long long oi = __shfl_xor_sync(0xffffffffu, bi, o);
-    if (ov > bv || (ov == bv && oi < bi)) {
-      bv = ov;
-      bi = oi;
-    }
-  }
+  for (int o = 16; o; o >>= 1)
+    argmax_take(__shfl_xor_sync(0xffffffffu, bv, o), __shfl_xor_sync(0xffffffffu, bi, o), bv, bi);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (lane == 0) {
     s_v[warp] = bv;
@@ -613,11 +605,32 @@ __global__ void argmax_pose_kernel(const float* __restrict__ scores, size_t U,
   __syncthreads();
   if (threadIdx.x == 0) {
     const int nw = (blockDim.x + 31) / 32;
-    for (int w = 1; w < nw; ++w)
-      if (s_v[w] > bv || (s_v[w] == bv && s_i[w] < bi)) {
-        bv = s_v[w];
-        bi = s_i[w];
-      }
+    for (int w = 1; w < nw; ++w) argmax_take(s_v[w], s_i[w], bv, bi);
+  }
+}
+
+__global__ void argmax_partial_kernel(const float* __restrict__ scores, size_t U, float* __restrict__ part_v,
+                                      unsigned long long* __restrict__ part_i) {
+  float bv = -INFINITY;
+  unsigned long long bi = ~0ull;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < U; i += (size_t)gridDim.x * blockDim.x)
+    argmax_take(scores[i], i, bv, bi);
+  block_argmax(bv, bi);
+  if (threadIdx.x == 0) {
+    part_v[blockIdx.x] = bv;
+    part_i[blockIdx.x] = bi;
+  }
+}
+
+__global__ void argmax_pose_kernel(const float* __restrict__ part_v, const unsigned long long* __restrict__ part_i,
+                                   uint32_t n_part, const float* __restrict__ scores,
+                                   const float* __restrict__ transforms, const float* __restrict__ trans,
+                                   float* __restrict__ best) {
+  float bv = -INFINITY;
+  unsigned long long bi = ~0ull;
+  for (uint32_t k = threadIdx.x; k < n_part; k += blockDim.x) argmax_take(part_v[k], part_i[k], bv, bi);
+  block_argmax(bv, bi);
+  if (threadIdx.x == 0) {
     if (bi == ~0ull) bi = 0;  // all scores NaN: first element, as max_element
     for (int k = 0; k < 16; ++k) best[k] = transforms[16 * bi + k];
     best[3] = trans[3 * bi];
@@ -884,9 +897,14 @@ size_t cluster_poses_gpu(Context& ctx, const Model& m, LookupState& st, float* b
     const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>(hc[1], (size_t)sm_count() * 8));
     cluster_tiled_kernel<<<grid, kClusterTile, 0, stream>>>(ta);
   }
-  argmax_pose_kernel<<<1, 1024, 0, stream>>>(a.scores, U, st.transforms.as<float>(), a.trans, best);
+  const unsigned n_part = grid_for(U, 256, 2);
+  float* part_v = grow<float>(st.argmax_v, n_part);
+  unsigned long long* part_i = grow<unsigned long long>(st.argmax_i, n_part);
+  argmax_partial_kernel<<<n_part, 256, 0, stream>>>(a.scores, U, part_v, part_i);
+  argmax_pose_kernel<<<1, 256, 0, stream>>>(part_v, part_i, n_part, a.scores, st.transforms.as<float>(), a.trans,
+                                            best);
   PPF_CUDA(cudaGetLastError());
-  ctx.launches += 2;
+  ctx.launches += 3;
   float h[20];
   PPF_CUDA(cudaMemcpyAsync(h, best, sizeof(h), cudaMemcpyDeviceToHost, stream));
   PPF_CUDA(cudaStreamSynchronize(stream));
