@@ -242,6 +242,7 @@ void init_context(Context& c, int device) {
   c.vote_smem_limit = optin - 2048;  // static shared memory of the vote kernel
   if (const char* e = std::getenv("PPF_B200_CHECKS")) c.checks = e[0] == '1';
   if (const char* e = std::getenv("PPF_B200_CLUSTER_SPLIT")) c.cluster_split = e[0] != '0';
+  if (const char* e = std::getenv("PPF_B200_CLUSTER_SQRT")) c.cluster_sqrt = e[0] == '1';
   if (const char* e = std::getenv("PPF_B200_TUNE")) c.tune = e[0] != '0';
   if (const char* e = std::getenv("PPF_B200_VOTE_SEGMENT")) {
     // a power of two from 256 to 65536 entries

@@ -60,6 +60,7 @@ struct Context {
   size_t launches = 0;      // kernels launched (running total)
   bool checks = false;      // self-checking kernels (PPF_B200_CHECKS=1)
   bool cluster_split = true; // exact-sum split clustering allowed (PPF_B200_CLUSTER_SPLIT=0: never)
+  bool cluster_sqrt = false; // PPF_B200_CLUSTER_SQRT=1: translation test with the square root
   ~Context();
 };
 

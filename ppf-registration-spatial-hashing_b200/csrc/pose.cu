@@ -271,12 +271,60 @@ __device__ __forceinline__ uint32_t quat_bucket(float4 q) {
 }
 
 // Sort key of each pose as a clustering target: its cell key, then its
-// rotation bucket, so the 32 targets of a warp hold similar rotations.
+// rotation bucket, then its quarter-cell of translation (4x4x4 sub-cells of
+// d_dist / 4), so the 32 targets of a warp hold similar rotations and, where
+// a rotation bucket is crowded, nearby translations.  54 bits.  On the bench's
+// pose-dense model the warp boxes then hold 9.0% of the neighbour poses,
+// against 13.7% with the rotation bucket alone.
+constexpr int kTargetKeyBits = 54;
 __global__ void target_keys_kernel(const uint32_t* __restrict__ sorted_keys, const float4* __restrict__ qs,
-                                   size_t U, unsigned long long* __restrict__ keys) {
+                                   const float4* __restrict__ tws, float sub_scale, size_t U,
+                                   unsigned long long* __restrict__ keys) {
   for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < U;
-       p += (size_t)gridDim.x * blockDim.x)
-    keys[p] = ((unsigned long long)sorted_keys[p] << 16) | quat_bucket(qs[p]);
+       p += (size_t)gridDim.x * blockDim.x) {
+    const float4 tw = tws[p];
+    const uint32_t sub = ((uint32_t)__float2int_rd(tw.x * sub_scale) & 3u) << 4 |
+                         ((uint32_t)__float2int_rd(tw.y * sub_scale) & 3u) << 2 |
+                         ((uint32_t)__float2int_rd(tw.z * sub_scale) & 3u);
+    keys[p] = ((unsigned long long)sorted_keys[p] << 22) | ((unsigned long long)quat_bucket(qs[p]) << 6) | sub;
+  }
+}
+
+// The translation test of the clustering kernels is sqrtf(|t - s|^2) < d.
+// sqrtf is non-decreasing in its argument wherever it is checked here, so the
+// test equals |t - s|^2 < x_star for x_star the smallest float whose sqrtf
+// reaches d, and the square root can be left out.  Every block finds x_star
+// by bisection over the float bit patterns with the device's own sqrtf (the
+// one the clustering kernels would call), then compares both forms of the
+// test on its share of the 2^21 + 1 floats around x_star; out[1] is set on
+// any disagreement (or a subnormal x_star, which ftz comparisons would flush),
+// and the kernels then keep the square root.  Further from x_star than 2^20
+// ulps the argument differs from x_star by more than 1/16 of it, far beyond
+// the error of the approximate square root, so both forms agree there too.
+constexpr uint32_t kDistWindow = 1u << 20;
+__global__ void dist_threshold_kernel(float d, uint32_t* __restrict__ out) {
+  __shared__ uint32_t s_star;
+  if (threadIdx.x == 0) {
+    uint32_t lo = 0u, hi = 0x7f800000u;  // sqrtf(0) < d <= sqrtf(inf) for finite d > 0
+    while (hi - lo > 1u) {
+      const uint32_t mid = lo + (hi - lo) / 2u;
+      if (sqrtf(__uint_as_float(mid)) < d) lo = mid;
+      else hi = mid;
+    }
+    s_star = hi;
+    if (blockIdx.x == 0) out[0] = hi;
+  }
+  __syncthreads();
+  const uint32_t star = s_star;
+  const float x_star = __uint_as_float(star);
+  const uint32_t first = star > kDistWindow ? star - kDistWindow : 0u;
+  const uint32_t last = min(star + kDistWindow, 0x7f800000u);
+  const uint32_t b = first + blockIdx.x * blockDim.x + threadIdx.x;
+  if (b <= last) {
+    const float x = __uint_as_float(b);
+    if ((sqrtf(x) < d) != (x < x_star)) atomicOr(out + 1, 1u);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && star < 0x00800000u) atomicOr(out + 1, 1u);
 }
 
 // Per cell run: its 27 neighbour runs (-1: none / the centre), the number of
@@ -326,10 +374,28 @@ struct TiledArgs {
   const float4* tws;
   float d_dist;
   float qmargin;  // quaternion half-width of the box filter (quat_margin)
+  float x_star;   // |t - s|^2 < x_star equals sqrtf(|t - s|^2) < d_dist (dist_threshold_kernel)
+  int use_x_star;
   int use_l1, use_avg;
   float* scores;
   float* trans;
 };
+
+// The reference's two tests for a source pose (rot_clustering_kernel,
+// src/cuda/kernel.cu:702-763): |8 (1 - q.s)| < rot_sq, and in L2 mode
+// sqrtf(|t - s|^2) < d_dist.  Multiplying by 8 is exact, so the first equals
+// |1 - q.s| < rot_sq / 8; the second uses the calibrated threshold when the
+// host found it valid.  The dot products round as the reference's.
+__device__ __forceinline__ bool cluster_match(const TiledArgs& a, float4 q, float3 t, float4 s, float4 sw,
+                                              float rot_sq8) {
+  bool ok = fabsf(1 - dot4(q, s)) < rot_sq8;
+  if (!a.use_l1) {
+    const float3 v = v3_sub(t, make_float3(sw.x, sw.y, sw.z));
+    const float d2 = dot3(v, v);
+    ok = ok && (a.use_x_star ? d2 < a.x_star : sqrtf(d2) < a.d_dist);
+  }
+  return ok;
+}
 
 __device__ __forceinline__ float warp_min(float v) {
 #pragma unroll
@@ -352,9 +418,9 @@ __device__ __forceinline__ float warp_max(float v) {
 // in L2 mode, translation components within 1.0001 d_dist.  It then runs the
 // reference's tests on the marked sources only, in ascending order, so every
 // target adds the same weights in the same order as the reference.
-__global__ void __launch_bounds__(kClusterTile) cluster_tiled_kernel(TiledArgs a) {
+__global__ void __launch_bounds__(kClusterTile, 5) cluster_tiled_kernel(TiledArgs a) {
   __shared__ float4 sq[kClusterTile], stw[kClusterTile];
-  const float rot_sq = PPF_ROT_THRESH * PPF_ROT_THRESH;
+  const float rot_sq8 = PPF_ROT_THRESH * PPF_ROT_THRESH * 0.125f;
   const int lane = threadIdx.x & 31;
   const float kQuatMargin = a.qmargin;
   const float t_margin = a.use_l1 ? INFINITY : a.d_dist * 1.0001f + 1e-6f;
@@ -434,15 +500,7 @@ __global__ void __launch_bounds__(kClusterTile) cluster_tiled_kernel(TiledArgs a
               swv[u] = stw[jj[u]];
             }
 #pragma unroll
-            for (int u = 0; u < 2; ++u) {
-              const float qd = fabsf(8 * (1 - dot4(q, sqv[u])));
-              bool ok = u < nj && qd < rot_sq;
-              if (!a.use_l1) {
-                const float nd = norm3(v3_sub(t, make_float3(swv[u].x, swv[u].y, swv[u].z)));
-                ok = ok && nd < a.d_dist;
-              }
-              pass[u] = ok;
-            }
+            for (int u = 0; u < 2; ++u) pass[u] = u < nj && cluster_match(a, q, t, sqv[u], swv[u], rot_sq8);
 #pragma unroll
             for (int u = 0; u < 2; ++u) {
               if (!pass[u]) continue;
@@ -511,7 +569,7 @@ __global__ void split_init_kernel(size_t U, const float* __restrict__ trans0, fl
 constexpr int kSplitBlock = 256;
 
 __global__ void __launch_bounds__(kSplitBlock) cluster_split_kernel(TiledArgs a) {
-  const float rot_sq = PPF_ROT_THRESH * PPF_ROT_THRESH;
+  const float rot_sq8 = PPF_ROT_THRESH * PPF_ROT_THRESH * 0.125f;
   const int lane = threadIdx.x & 31;
   const float kQuatMargin = a.qmargin;  // as cluster_tiled_kernel
   const float t_margin = a.use_l1 ? INFINITY : a.d_dist * 1.0001f + 1e-6f;
@@ -571,9 +629,7 @@ __global__ void __launch_bounds__(kSplitBlock) cluster_split_kernel(TiledArgs a)
                                      __shfl_sync(0xffffffffu, sj.z, src), __shfl_sync(0xffffffffu, sj.w, src));
         const float4 sw = make_float4(__shfl_sync(0xffffffffu, wj.x, src), __shfl_sync(0xffffffffu, wj.y, src),
                                       __shfl_sync(0xffffffffu, wj.z, src), __shfl_sync(0xffffffffu, wj.w, src));
-        bool ok = valid && fabsf(8 * (1 - dot4(q, s))) < rot_sq;
-        if (!a.use_l1) ok = ok && norm3(v3_sub(t, make_float3(sw.x, sw.y, sw.z))) < a.d_dist;
-        if (ok) c += sw.w;
+        if (valid && cluster_match(a, q, t, s, sw, rot_sq8)) c += sw.w;
       }
     }
     if (valid && c != 0.f) atomicAdd(&a.scores[a.map[p]], c);
@@ -811,9 +867,16 @@ size_t cluster_poses_gpu(Context& ctx, const Model& m, LookupState& st, float* b
   const bool may_split = ctx.cluster_split && !m.use_averaged_clusters;
   uint32_t* item_off32 = may_split ? grow<uint32_t>(st.item_off32, Kc + 1) : nullptr;
   // counters: [0] mixed cells, [1] tiles, [2] split items, [3] non-integer
-  // weight, [4..5] sum of |weight|, [6] largest squared quaternion norm
-  PPF_CUDA(cudaMemsetAsync(ctx.counters.ptr, 0, 28, stream));
+  // weight, [4..5] sum of |weight|, [6] largest squared quaternion norm,
+  // [7] x_star of the translation test, [8] x_star unusable
+  PPF_CUDA(cudaMemsetAsync(ctx.counters.ptr, 0, 36, stream));
   uint32_t* mixed = ctx.counters.as<uint32_t>();
+  const float d_dist = m.t.d_dist;
+  const bool calibrate = !m.use_l1_norm && d_dist > 0.f && std::isfinite(d_dist);
+  if (calibrate) {
+    dist_threshold_kernel<<<(2 * kDistWindow + 1 + 255) / 256, 256, 0, stream>>>(d_dist, mixed + 7);
+    ctx.launches++;
+  }
   gather_sorted_kernel<<<grid_for(U, 256), 256, 0, stream>>>(map, U, a.quats, a.trans0, a.weighted, qs, tws,
                                                               mixed + 6);
   mixed_cells_kernel<<<grid_for(U, 256), 256, 0, stream>>>(ck, map, st.cells3.as<int4>(), U, mixed);
@@ -827,12 +890,16 @@ size_t cluster_poses_gpu(Context& ctx, const Model& m, LookupState& st, float* b
                                                               reinterpret_cast<unsigned long long*>(mixed + 4));
     ctx.launches += 2;
   }
-  uint32_t hc[7];
+  uint32_t hc[9];
   PPF_CUDA(cudaMemcpyAsync(hc, mixed, sizeof(hc), cudaMemcpyDeviceToHost, stream));
   PPF_CUDA(cudaStreamSynchronize(stream));
-  float max_qq;
+  float max_qq, x_star;
   std::memcpy(&max_qq, hc + 6, sizeof(max_qq));
+  std::memcpy(&x_star, hc + 7, sizeof(x_star));
   const float qmargin = quat_margin(max_qq);
+  const int use_x_star = calibrate && !hc[8] && !ctx.cluster_sqrt;
+  // quarter-cell translation bins of the target order
+  const float sub_scale = d_dist > 0.f && std::isfinite(d_dist) ? 4.f / d_dist : 0.f;
   const unsigned long long abs_sum = hc[4] | ((unsigned long long)hc[5] << 32);
   const bool split = may_split && !hc[0] && !hc[3] && abs_sum < (1ull << 24) - 1;
   st.cluster_path = split ? 3 : hc[0] ? 2 : 1;
@@ -840,9 +907,9 @@ size_t cluster_poses_gpu(Context& ctx, const Model& m, LookupState& st, float* b
     // targets of each cell ordered by rotation bucket, as below
     unsigned long long* tkeys = grow<unsigned long long>(st.tmp64, U);
     uint32_t* tperm = grow<uint32_t>(st.tperm, U);
-    target_keys_kernel<<<grid_for(U, 256), 256, 0, stream>>>(ck, qs, U, tkeys);
+    target_keys_kernel<<<grid_for(U, 256), 256, 0, stream>>>(ck, qs, tws, sub_scale, U, tkeys);
     const size_t l1 = ctx.sort64.launches();
-    ctx.sort64.sort(tkeys, tperm, true, U, 0, 48, stream, ctx.flags.as<uint32_t>());
+    ctx.sort64.sort(tkeys, tperm, true, U, 0, kTargetKeyBits, stream, ctx.flags.as<uint32_t>());
     ctx.launches += 1 + ctx.sort64.launches() - l1;
     split_init_kernel<<<grid_for(U, 256), 256, 0, stream>>>(U, a.trans0, a.scores, a.trans);
     TiledArgs ta;
@@ -858,6 +925,8 @@ size_t cluster_poses_gpu(Context& ctx, const Model& m, LookupState& st, float* b
     ta.tws = tws;
     ta.d_dist = m.t.d_dist;
     ta.qmargin = qmargin;
+    ta.x_star = x_star;
+    ta.use_x_star = use_x_star;
     ta.use_l1 = m.use_l1_norm;
     ta.use_avg = 0;
     ta.scores = a.scores;
@@ -872,10 +941,10 @@ size_t cluster_poses_gpu(Context& ctx, const Model& m, LookupState& st, float* b
     // targets of each cell ordered by rotation bucket
     unsigned long long* tkeys = grow<unsigned long long>(st.tmp64, U);
     uint32_t* tperm = grow<uint32_t>(st.tperm, U);
-    target_keys_kernel<<<grid_for(U, 256), 256, 0, stream>>>(ck, qs, U, tkeys);
+    target_keys_kernel<<<grid_for(U, 256), 256, 0, stream>>>(ck, qs, tws, sub_scale, U, tkeys);
     ctx.launches++;
     const size_t l1 = ctx.sort64.launches();
-    ctx.sort64.sort(tkeys, tperm, true, U, 0, 48, stream, ctx.flags.as<uint32_t>());
+    ctx.sort64.sort(tkeys, tperm, true, U, 0, kTargetKeyBits, stream, ctx.flags.as<uint32_t>());
     ctx.launches += ctx.sort64.launches() - l1;
     TiledArgs ta;
     ta.tperm = tperm;
@@ -890,6 +959,8 @@ size_t cluster_poses_gpu(Context& ctx, const Model& m, LookupState& st, float* b
     ta.tws = tws;
     ta.d_dist = m.t.d_dist;
     ta.qmargin = qmargin;
+    ta.x_star = x_star;
+    ta.use_x_star = use_x_star;
     ta.use_l1 = m.use_l1_norm;
     ta.use_avg = m.use_averaged_clusters;
     ta.scores = a.scores;

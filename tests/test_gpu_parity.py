@@ -379,6 +379,36 @@ def test_split_clustering_equals_ordered(pkg, ctx, ref_gpu, monkeypatch):
         assert _same(pa.ravel(), R["pose"].ravel())
 
 
+def test_translation_threshold_equals_square_root(pkg, ctx, ref_gpu, monkeypatch):
+    """The clustering kernels compare |t - s|^2 with a device-calibrated
+    threshold instead of sqrtf(|t - s|^2) with d_dist.  With the square root
+    forced back (PPF_B200_CLUSTER_SQRT=1) the ordered, split and averaged paths
+    give the same scores, translations and poses bit for bit, equal to the
+    reference's kernels, on models whose poses crowd each other's cells."""
+    spec = pkg.synthetic.config_plain(seed=163, n_model=1100, n_plane=2200, n_box=700)
+    m, s, d = spec.models[0], spec.scene, spec.d_dists[0]
+    monkeypatch.setenv("PPF_B200_CLUSTER_SQRT", "1")
+    sctx = pkg.Context(0)
+    cases = [({}, None, 3), ({}, 0.5, 1), ({"use_averaged_clusters": True}, None, 1)]
+    for kw, w, path in cases:
+        out = []
+        for c in (ctx, sctx):
+            model = pkg.Model(m, d, 0.3, context=c, **kw)
+            if w is not None:
+                model.SetModelPointVoteWeights(np.full(len(m), w, np.float32))
+            pose = model.ppf_lookup(pkg.Scene(s, d, 5, context=c)).copy()
+            assert model.stats["cluster_path"] == path, (kw, w)
+            out.append((pose, model.get_cluster_state(), model.stats["max_idx"]))
+        (pa, sa, ia), (pb, sb, ib) = out
+        for x, y in zip(sa, sb):
+            assert _same(x, y), (kw, w)
+        assert ia == ib and _same(pa.ravel(), pb.ravel()), (kw, w)
+        if w is None and not kw:  # the reference races in averaged mode
+            R = ref_gpu.lookup((m.points, m.normals), (s.points, s.normals), d, 5, 0.3)
+            assert _same(sa[2], R["scores"])
+            assert _same(pa.ravel(), R["pose"].ravel())
+
+
 def test_cluster_path_selection(pkg, ctx):
     """Non-integer weights, integer weights whose total reaches 2^24 and
     averaged clusters keep the ordered sums."""
