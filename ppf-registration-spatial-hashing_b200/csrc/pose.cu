@@ -11,6 +11,21 @@
 namespace ppf {
 namespace {
 
+// The rotation and translation tests' dot products with the contraction
+// written out, so that the rounding does not depend on how the compiler
+// contracts the expression where it is inlined: y*y' rounded, x*x' fused onto
+// it, then z*z' and w*w' fused in turn.  This is the rounding of the
+// reference's dot() in its clustering kernel (src/cuda/kernel.cu:737-743, as
+// nvcc contracts x*x' + y*y' + z*z' + w*w'): on the bench's 31 M poses every
+// score equals theirs, while fusing y*y' onto a rounded x*x' instead, in
+// either sum, changed scores (up to 950 of them).
+__device__ __forceinline__ float dot4_fused(float4 a, float4 b) {
+  return fmaf(a.w, b.w, fmaf(a.z, b.z, fmaf(a.x, b.x, __fmul_rn(a.y, b.y))));
+}
+__device__ __forceinline__ float dot3_fused(float3 a) {
+  return fmaf(a.z, a.z, fmaf(a.x, a.x, __fmul_rn(a.y, a.y)));
+}
+
 // Keep candidates with count > min_votecount (compared in float, as the
 // reference's count_if lambda does, src/cuda/model.cu:164-167).
 __global__ void filter_kernel(const unsigned long long* __restrict__ code,
@@ -187,11 +202,11 @@ __global__ void cluster_kernel(ClusterArgs a) {
         uint32_t j = a.map[f + e];
         float w = a.weighted[j];
         float4 qj = make_float4(a.quats[4 * j], a.quats[4 * j + 1], a.quats[4 * j + 2], a.quats[4 * j + 3]);
-        float qd = fabsf(8 * (1 - dot4(q, qj)));
+        float qd = fabsf(8 * (1 - dot4_fused(q, qj)));
         if (qd < rot_sq) {
           float3 tj = make_float3(a.trans0[3 * j], a.trans0[3 * j + 1], a.trans0[3 * j + 2]);
           if (!a.use_l1) {
-            float nd = norm3(v3_sub(t, tj));
+            float nd = sqrtf(dot3_fused(v3_sub(t, tj)));
             if (!(nd < a.d_dist)) continue;
           }
           if (a.use_avg) {
@@ -210,14 +225,7 @@ __global__ void cluster_kernel(ClusterArgs a) {
   }
 }
 
-// ---- cell-major clustering ------------------------------------------------
-// The same scores as cluster_kernel, computed per (cell run, tile of 256
-// target poses): the poses of each neighbour cell run are streamed through
-// shared memory once per tile and tested by every target of the tile.  Each
-// target still visits its neighbours in the reference's order (neighbour
-// b = 0..26, then run order), so sums and running averages round the same.
-
-constexpr int kClusterTile = 256;
+constexpr int kGroup = 32;  // clustering targets per warp
 
 // Also folds the largest squared norm of a finite quaternion into *max_qq
 // (float bits; non-negative floats order as their bits).
@@ -328,12 +336,12 @@ __global__ void dist_threshold_kernel(float d, uint32_t* __restrict__ out) {
 }
 
 // Per cell run: its 27 neighbour runs (-1: none / the centre), the number of
-// target tiles and, if items32 is set, the number of split items (32-target
+// 32-target groups and, if items32 is set, the number of split items (32-target
 // tiles x 27 neighbours).
 __global__ void run_adjacency_kernel(const uint32_t* __restrict__ first, const uint32_t* __restrict__ count,
                                      size_t Kc, const uint32_t* __restrict__ map,
                                      const int4* __restrict__ cells3, const uint32_t* __restrict__ uniq,
-                                     int* __restrict__ adjrun, uint32_t* __restrict__ tiles,
+                                     int* __restrict__ adjrun, uint32_t* __restrict__ groups,
                                      uint32_t* __restrict__ items32) {
   for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < Kc;
        r += (size_t)gridDim.x * blockDim.x) {
@@ -356,12 +364,12 @@ __global__ void run_adjacency_kernel(const uint32_t* __restrict__ first, const u
           }
           adjrun[r * 27 + b] = run;
         }
-    tiles[r] = (n + kClusterTile - 1) / kClusterTile;
+    groups[r] = (n + kGroup - 1) / kGroup;
     if (items32) items32[r] = (n + 31) / 32 * 27;
   }
 }
 
-struct TiledArgs {
+struct GroupArgs {
   const uint32_t* first;
   const uint32_t* count;
   const uint32_t* map;
@@ -386,15 +394,27 @@ struct TiledArgs {
 // sqrtf(|t - s|^2) < d_dist.  Multiplying by 8 is exact, so the first equals
 // |1 - q.s| < rot_sq / 8; the second uses the calibrated threshold when the
 // host found it valid.  The dot products round as the reference's.
-__device__ __forceinline__ bool cluster_match(const TiledArgs& a, float4 q, float3 t, float4 s, float4 sw,
-                                              float rot_sq8) {
-  bool ok = fabsf(1 - dot4(q, s)) < rot_sq8;
-  if (!a.use_l1) {
+// Translation test of a clustering launch: none (L1 mode), the calibrated
+// threshold, or the square root.
+enum TransTest : int { kTransNone = 0, kTransThreshold = 1, kTransSqrt = 2 };
+
+template <int TT>
+__device__ __forceinline__ bool cluster_match_t(const GroupArgs& a, float4 q, float3 t, float4 s, float4 sw,
+                                                float rot_sq8) {
+  bool ok = fabsf(1 - dot4_fused(q, s)) < rot_sq8;
+  if (TT != kTransNone) {
     const float3 v = v3_sub(t, make_float3(sw.x, sw.y, sw.z));
-    const float d2 = dot3(v, v);
-    ok = ok && (a.use_x_star ? d2 < a.x_star : sqrtf(d2) < a.d_dist);
+    const float d2 = dot3_fused(v);
+    ok = ok && (TT == kTransThreshold ? d2 < a.x_star : sqrtf(d2) < a.d_dist);
   }
   return ok;
+}
+
+__device__ __forceinline__ bool cluster_match(const GroupArgs& a, float4 q, float3 t, float4 s, float4 sw,
+                                              float rot_sq8) {
+  return a.use_l1 ? cluster_match_t<kTransNone>(a, q, t, s, sw, rot_sq8)
+         : a.use_x_star ? cluster_match_t<kTransThreshold>(a, q, t, s, sw, rot_sq8)
+                        : cluster_match_t<kTransSqrt>(a, q, t, s, sw, rot_sq8);
 }
 
 __device__ __forceinline__ float warp_min(float v) {
@@ -408,121 +428,175 @@ __device__ __forceinline__ float warp_max(float v) {
   return v;
 }
 
+// ---- warp-group clustering -------------------------------------------------
 // Scores of rot_clustering_kernel (src/cuda/kernel.cu:702-763), cell-major.
-// A block takes a tile of up to 256 targets of one cell, ordered by rotation
-// bucket, and streams the poses of the cell's neighbour cells through shared
-// memory in the reference's order (neighbour b = 0..26, then position).  Each
-// warp first marks, with one ballot per 32 sources, the sources inside a box
-// around its targets: quaternion components within quat_margin of some
-// target's (about 0.21: the rotation test bounds the quaternion distance) and,
-// in L2 mode, translation components within 1.0001 d_dist.  It then runs the
-// reference's tests on the marked sources only, in ascending order, so every
-// target adds the same weights in the same order as the reference.
-__global__ void __launch_bounds__(kClusterTile, 5) cluster_tiled_kernel(TiledArgs a) {
-  __shared__ float4 sq[kClusterTile], stw[kClusterTile];
+// A warp takes 32 targets of one cell (a group; targets ordered by rotation
+// bucket, then quarter-cell) and streams the poses of the cell's neighbour
+// cells, 32 at a time, into a private ring of kRingStages chunks in shared
+// memory with cp.async, kRingStages - 1 chunks ahead of its tests.  For each
+// chunk it marks, with one ballot, the sources inside a box around its
+// targets: quaternion components within quat_margin of some target's (about
+// 0.21: the rotation test bounds the quaternion distance) and, in L2 mode,
+// translation components within 1.0001 d_dist.  It then runs the reference's
+// tests on the marked sources only, in ascending order.  Sources are visited
+// in the reference's order (neighbour b = 0..26, then position), so every
+// target adds the same weights in the same order as the reference.  No block
+// barrier couples the warps of a block.
+
+constexpr int kWarpBlock = 128;  // threads per block: independent warps
+constexpr int kRingStages = 4;
+
+// Position in a group's stream of source chunks: neighbour b, offset o into
+// that neighbour run [f, f + n).
+struct ChunkPos {
+  int b;
+  uint32_t o, f, n;
+};
+
+// Advances to the next chunk of 32 sources; false past the last neighbour.
+__device__ __forceinline__ bool next_chunk(const GroupArgs& a, size_t r, ChunkPos& c) {
+  c.o += 32u;
+  while (c.o >= c.n) {
+    if (++c.b >= 27) return false;
+    const int nr = a.adjrun[r * 27 + c.b];
+    if (nr < 0) continue;
+    c.f = a.first[nr];
+    c.n = a.count[nr];
+    c.o = 0u;
+  }
+  return true;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+template <bool AVG, int TT>
+__global__ void __launch_bounds__(kWarpBlock, 8) cluster_warp_kernel(GroupArgs a) {
+  __shared__ float4 ring[kWarpBlock / 32][kRingStages][2][32];
+  __shared__ float4 marked[kWarpBlock / 32][2][32];
+  __shared__ uint32_t ring_len[kWarpBlock / 32][kRingStages];
   const float rot_sq8 = PPF_ROT_THRESH * PPF_ROT_THRESH * 0.125f;
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t item = blockIdx.x * (kWarpBlock / 32) + warp;
+  if (item >= a.n_items) return;  // uniform over the warp
+  size_t lo = 0, hi = a.Kc;  // run r with item_off[r] <= item < item_off[r + 1]
+  while (hi - lo > 1) {
+    size_t mid = (lo + hi) >> 1;
+    if (a.item_off[mid] <= item) lo = mid;
+    else hi = mid;
+  }
+  const size_t r = lo;
   const float kQuatMargin = a.qmargin;
-  const float t_margin = a.use_l1 ? INFINITY : a.d_dist * 1.0001f + 1e-6f;
-  for (uint32_t item = blockIdx.x; item < a.n_items; item += gridDim.x) {
-    size_t lo = 0, hi = a.Kc;  // run r with item_off[r] <= item < item_off[r + 1]
-    while (hi - lo > 1) {
-      size_t mid = (lo + hi) >> 1;
-      if (a.item_off[mid] <= item) lo = mid;
-      else hi = mid;
+  const float t_margin = a.d_dist * 1.0001f + 1e-6f;
+  const uint32_t slot = a.first[r] + (item - a.item_off[r]) * kGroup + lane;
+  const bool valid = slot < a.first[r] + a.count[r];
+  const uint32_t p = valid ? a.tperm[slot] : 0u;
+  // a lane without a target keeps q = 0, which fails the rotation test
+  float4 q = make_float4(0, 0, 0, 0), tw = make_float4(0, 0, 0, 0);
+  if (valid) {
+    q = a.qs[p];
+    tw = a.tws[p];
+  }
+  const float3 t = make_float3(tw.x, tw.y, tw.z);
+  const float4 qlo = make_float4(warp_min(valid ? q.x : INFINITY) - kQuatMargin,
+                                 warp_min(valid ? q.y : INFINITY) - kQuatMargin,
+                                 warp_min(valid ? q.z : INFINITY) - kQuatMargin,
+                                 warp_min(valid ? q.w : INFINITY) - kQuatMargin);
+  const float4 qhi = make_float4(warp_max(valid ? q.x : -INFINITY) + kQuatMargin,
+                                 warp_max(valid ? q.y : -INFINITY) + kQuatMargin,
+                                 warp_max(valid ? q.z : -INFINITY) + kQuatMargin,
+                                 warp_max(valid ? q.w : -INFINITY) + kQuatMargin);
+  float3 tlo = make_float3(0, 0, 0), thi = make_float3(0, 0, 0);
+  if (TT != kTransNone) {
+    tlo = make_float3(warp_min(valid ? t.x : INFINITY) - t_margin, warp_min(valid ? t.y : INFINITY) - t_margin,
+                      warp_min(valid ? t.z : INFINITY) - t_margin);
+    thi = make_float3(warp_max(valid ? t.x : -INFINITY) + t_margin, warp_max(valid ? t.y : -INFINITY) + t_margin,
+                      warp_max(valid ? t.z : -INFINITY) + t_margin);
+  }
+  float4(*const wr)[2][32] = ring[warp];
+  float4(*const mk)[32] = marked[warp];
+  uint32_t* const wm = ring_len[warp];
+  // The producer walks the chunk stream kRingStages - 1 chunks ahead of the
+  // tests and records each chunk's length; it commits one cp.async group per
+  // step (empty past the end), so wait_group<kRingStages - 1> leaves the
+  // chunk under test complete.
+  ChunkPos pc{-1, 0u, 0u, 0u};
+  bool more = next_chunk(a, r, pc);
+  uint32_t issued = 0;
+  auto produce = [&]() {
+    if (more) {
+      const uint32_t k = issued % kRingStages;
+      if (pc.o + lane < pc.n) {
+        cp_async16(&wr[k][0][lane], a.qs + pc.f + pc.o + lane);
+        cp_async16(&wr[k][1][lane], a.tws + pc.f + pc.o + lane);
+      }
+      if (lane == 0) wm[k] = min(32u, pc.n - pc.o);
+      ++issued;
+      more = next_chunk(a, r, pc);
     }
-    const size_t r = lo;
-    const uint32_t slot = a.first[r] + (item - a.item_off[r]) * kClusterTile + threadIdx.x;
-    const bool valid = slot < a.first[r] + a.count[r];
-    const uint32_t p = valid ? a.tperm[slot] : 0u;
-    float4 q = make_float4(0, 0, 0, 0), tw = make_float4(0, 0, 0, 0);
-    if (valid) {
-      q = a.qs[p];
-      tw = a.tws[p];
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int s = 0; s < kRingStages - 1; ++s) produce();
+  const uint32_t lanes_below = (1u << lane) - 1u;
+  float c = 1;
+  float3 to = t;
+  for (uint32_t used = 0; used < issued; ++used) {
+    produce();
+    cp_async_wait<kRingStages - 1>();
+    __syncwarp();
+    const uint32_t k = used % kRingStages;
+    bool in = false;
+    float4 sj, wj;
+    if ((uint32_t)lane < wm[k]) {
+      sj = wr[k][0][lane];
+      wj = wr[k][1][lane];
+      in = sj.x >= qlo.x && sj.x <= qhi.x && sj.y >= qlo.y && sj.y <= qhi.y && sj.z >= qlo.z && sj.z <= qhi.z &&
+           sj.w >= qlo.w && sj.w <= qhi.w;
+      if (TT != kTransNone)
+        in = in && wj.x >= tlo.x && wj.x <= thi.x && wj.y >= tlo.y && wj.y <= thi.y && wj.z >= tlo.z &&
+             wj.z <= thi.z;
     }
-    const float3 t = make_float3(tw.x, tw.y, tw.z);
-    // the warp's box (empty for a warp without targets)
-    const float4 qlo = make_float4(warp_min(valid ? q.x : INFINITY) - kQuatMargin,
-                                   warp_min(valid ? q.y : INFINITY) - kQuatMargin,
-                                   warp_min(valid ? q.z : INFINITY) - kQuatMargin,
-                                   warp_min(valid ? q.w : INFINITY) - kQuatMargin);
-    const float4 qhi = make_float4(warp_max(valid ? q.x : -INFINITY) + kQuatMargin,
-                                   warp_max(valid ? q.y : -INFINITY) + kQuatMargin,
-                                   warp_max(valid ? q.z : -INFINITY) + kQuatMargin,
-                                   warp_max(valid ? q.w : -INFINITY) + kQuatMargin);
-    const float3 tlo = make_float3(warp_min(valid ? t.x : INFINITY) - t_margin,
-                                   warp_min(valid ? t.y : INFINITY) - t_margin,
-                                   warp_min(valid ? t.z : INFINITY) - t_margin);
-    const float3 thi = make_float3(warp_max(valid ? t.x : -INFINITY) + t_margin,
-                                   warp_max(valid ? t.y : -INFINITY) + t_margin,
-                                   warp_max(valid ? t.z : -INFINITY) + t_margin);
-    float c = 1;
-    float3 to = t;
-    for (int b = 0; b < 27; ++b) {
-      const int nr = a.adjrun[r * 27 + b];
-      if (nr < 0) continue;
-      const uint32_t f = a.first[nr], n = a.count[nr];
-      for (uint32_t s0 = 0; s0 < n; s0 += kClusterTile) {
-        __syncthreads();
-        if (s0 + threadIdx.x < n) {
-          sq[threadIdx.x] = a.qs[f + s0 + threadIdx.x];
-          stw[threadIdx.x] = a.tws[f + s0 + threadIdx.x];
-        }
-        __syncthreads();
-        const uint32_t m = min((uint32_t)kClusterTile, n - s0);
-        for (uint32_t j0 = 0; j0 < m; j0 += 32) {
-          const uint32_t jl = j0 + lane;
-          bool in = false;
-          if (jl < m) {
-            const float4 sj = sq[jl], wj = stw[jl];
-            in = sj.x >= qlo.x && sj.x <= qhi.x && sj.y >= qlo.y && sj.y <= qhi.y && sj.z >= qlo.z &&
-                 sj.z <= qhi.z && sj.w >= qlo.w && sj.w <= qhi.w && wj.x >= tlo.x && wj.x <= thi.x &&
-                 wj.y >= tlo.y && wj.y <= thi.y && wj.z >= tlo.z && wj.z <= thi.z;
+    const uint32_t mask = __ballot_sync(0xffffffffu, in);
+    if (mask) {  // uniform
+      // the marked sources, in ascending position, as one list
+      if (in) {
+        const uint32_t at = __popc(mask & lanes_below);
+        mk[0][at] = sj;
+        mk[1][at] = wj;
+      }
+      __syncwarp();
+      const int n = __popc(mask);
+#pragma unroll 2
+      for (int e = 0; e < n; ++e) {
+        const float4 sv = mk[0][e], wv = mk[1][e];
+        if (cluster_match_t<TT>(a, q, t, sv, wv, rot_sq8)) {
+          if (AVG) {
+            const float3 tj = make_float3(wv.x, wv.y, wv.z);
+            to = v3_scale(c, to);
+            to = v3_add(to, v3_scale(wv.w, tj));
+            to = v3_scale(1 / (c + wv.w), to);
           }
-          uint32_t mask = __ballot_sync(0xffffffffu, in);
-          while (mask) {
-            // up to 2 marked sources at a time: their tests are independent,
-            // their weights are added in ascending order as before
-            uint32_t jj[2];
-            int nj = 0;
-#pragma unroll
-            for (int u = 0; u < 2; ++u) {
-              jj[u] = j0 + (mask ? (uint32_t)(__ffs(mask) - 1) : 0u);
-              nj += mask ? 1 : 0;
-              mask &= mask - 1;
-            }
-            if (!valid) continue;
-            float4 sqv[2], swv[2];
-            bool pass[2];
-#pragma unroll
-            for (int u = 0; u < 2; ++u) {
-              sqv[u] = sq[jj[u]];
-              swv[u] = stw[jj[u]];
-            }
-#pragma unroll
-            for (int u = 0; u < 2; ++u) pass[u] = u < nj && cluster_match(a, q, t, sqv[u], swv[u], rot_sq8);
-#pragma unroll
-            for (int u = 0; u < 2; ++u) {
-              if (!pass[u]) continue;
-              const float3 tj = make_float3(swv[u].x, swv[u].y, swv[u].z);
-              if (a.use_avg) {
-                to = v3_scale(c, to);
-                to = v3_add(to, v3_scale(swv[u].w, tj));
-                to = v3_scale(1 / (c + swv[u].w), to);
-              }
-              c += swv[u].w;
-            }
-          }
+          c += wv.w;
         }
       }
     }
-    if (valid) {
-      const uint32_t o = a.map[p];
-      a.scores[o] = c;
-      a.trans[3 * o] = to.x;
-      a.trans[3 * o + 1] = to.y;
-      a.trans[3 * o + 2] = to.z;
-    }
+    __syncwarp();  // every lane is done with this slot and the list before both are refilled
+  }
+  cp_async_wait<0>();
+  if (valid) {
+    const uint32_t o = a.map[p];
+    a.scores[o] = c;
+    a.trans[3 * o] = to.x;
+    a.trans[3 * o + 1] = to.y;
+    a.trans[3 * o + 2] = to.z;
   }
 }
 
@@ -532,7 +606,7 @@ __global__ void __launch_bounds__(kClusterTile, 5) cluster_tiled_kernel(TiledArg
 // target's score is the same whatever the order of its additions.  The work
 // can then be split per (32-target tile, neighbour cell): each warp tests one
 // neighbour cell's poses against its 32 targets, in the same box-filtered way
-// as cluster_tiled_kernel, and adds its partial sum with a float atomic.  A
+// as cluster_warp_kernel, and adds its partial sum with a float atomic.  A
 // lookup with few poses then spreads over up to 27x more warps.
 
 // nonint: some weight is not an integer below 2^24 (or is NaN); abs_sum: the
@@ -568,10 +642,10 @@ __global__ void split_init_kernel(size_t U, const float* __restrict__ trans0, fl
 
 constexpr int kSplitBlock = 256;
 
-__global__ void __launch_bounds__(kSplitBlock) cluster_split_kernel(TiledArgs a) {
+__global__ void __launch_bounds__(kSplitBlock) cluster_split_kernel(GroupArgs a) {
   const float rot_sq8 = PPF_ROT_THRESH * PPF_ROT_THRESH * 0.125f;
   const int lane = threadIdx.x & 31;
-  const float kQuatMargin = a.qmargin;  // as cluster_tiled_kernel
+  const float kQuatMargin = a.qmargin;  // as cluster_warp_kernel
   const float t_margin = a.use_l1 ? INFINITY : a.d_dist * 1.0001f + 1e-6f;
   const uint32_t n_warps = gridDim.x * (kSplitBlock / 32);
   for (uint32_t item = blockIdx.x * (kSplitBlock / 32) + (threadIdx.x >> 5); item < a.n_items;
@@ -856,7 +930,7 @@ size_t cluster_poses_gpu(Context& ctx, const Model& m, LookupState& st, float* b
   a.use_avg = m.use_averaged_clusters;
   a.scores = st.scores.as<float>();
   a.trans = st.trans.as<float>();
-  // cell-major tiled scores; per-pose neighbour lists only if two different
+  // cell-major group scores; per-pose neighbour lists only if two different
   // cells share a hash inside one run
   float4* qs = grow<float4>(st.qs, U);
   float4* tws = grow<float4>(st.tws, U);
@@ -912,7 +986,7 @@ size_t cluster_poses_gpu(Context& ctx, const Model& m, LookupState& st, float* b
     ctx.sort64.sort(tkeys, tperm, true, U, 0, kTargetKeyBits, stream, ctx.flags.as<uint32_t>());
     ctx.launches += 1 + ctx.sort64.launches() - l1;
     split_init_kernel<<<grid_for(U, 256), 256, 0, stream>>>(U, a.trans0, a.scores, a.trans);
-    TiledArgs ta;
+    GroupArgs ta;
     ta.tperm = tperm;
     ta.first = fi;
     ta.count = ct;
@@ -946,7 +1020,7 @@ size_t cluster_poses_gpu(Context& ctx, const Model& m, LookupState& st, float* b
     const size_t l1 = ctx.sort64.launches();
     ctx.sort64.sort(tkeys, tperm, true, U, 0, kTargetKeyBits, stream, ctx.flags.as<uint32_t>());
     ctx.launches += ctx.sort64.launches() - l1;
-    TiledArgs ta;
+    GroupArgs ta;
     ta.tperm = tperm;
     ta.first = fi;
     ta.count = ct;
@@ -965,8 +1039,19 @@ size_t cluster_poses_gpu(Context& ctx, const Model& m, LookupState& st, float* b
     ta.use_avg = m.use_averaged_clusters;
     ta.scores = a.scores;
     ta.trans = a.trans;
-    const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>(hc[1], (size_t)sm_count() * 8));
-    cluster_tiled_kernel<<<grid, kClusterTile, 0, stream>>>(ta);
+    const size_t blocks = (hc[1] + kWarpBlock / 32 - 1) / (kWarpBlock / 32);
+    const unsigned grid = (unsigned)std::max<size_t>(1, blocks);
+    const int tt = m.use_l1_norm ? kTransNone : use_x_star ? kTransThreshold : kTransSqrt;
+    auto launch = [&](auto kernel) { kernel<<<grid, kWarpBlock, 0, stream>>>(ta); };
+    if (m.use_averaged_clusters) {
+      if (tt == kTransNone) launch(cluster_warp_kernel<true, kTransNone>);
+      else if (tt == kTransThreshold) launch(cluster_warp_kernel<true, kTransThreshold>);
+      else launch(cluster_warp_kernel<true, kTransSqrt>);
+    } else {
+      if (tt == kTransNone) launch(cluster_warp_kernel<false, kTransNone>);
+      else if (tt == kTransThreshold) launch(cluster_warp_kernel<false, kTransThreshold>);
+      else launch(cluster_warp_kernel<false, kTransSqrt>);
+    }
   }
   const unsigned n_part = grid_for(U, 256, 2);
   float* part_v = grow<float>(st.argmax_v, n_part);

@@ -15,6 +15,9 @@
 * A model of the bench workload (5711 points: four m_r chunks of the vote
   accumulator) against a cut of the bench scene, bit for bit against the
   reference's kernels.
+* The bench's pose-dense model against the whole bench scene at
+  ref_point_df 5: the engine's 31 M kept votes through the reference's
+  post-vote kernels, every float output bit for bit.
 * The bench scene itself (60000 points) against each of its four models at
   ref_point_df 2000 (30 scene reference points): every vote cell compared
   with the CPU oracle.  Host libm and IEEE division differ from the device's
@@ -159,6 +162,29 @@ def test_bench_model_four_chunks_against_reference_kernels(pkg, ctx, ref_gpu, be
     _compare_lookup(mine, ref_gpu.post(mc, cut, d, kc, kk), kc, kk)
     _record("bench_model0_cut", n_votes=R["n_votes"], reference_vote_ms=R["elapsed_ms"],
             engine_vote_ms=mine["stats"]["vote_ms"])
+
+
+def test_bench_pose_dense_model_post_vote_against_reference_kernels(pkg, ctx, ref_gpu, bench_spec):
+    """The bench's pose-dense model (2x3 spheres on a slab, 3047 points)
+    against the whole 60000-point scene at the bench's ref_point_df 5: 31 M
+    kept votes whose translation cells hold up to 37,000 poses.  The engine's
+    kept votes go through the reference's pose, weight and clustering kernels,
+    and every transform, quaternion, score (float sums near 1e8, where the
+    order of the additions decides the rounding), translation, the best index
+    and the best pose equal the engine's bit for bit."""
+    spec = bench_spec
+    k = 3
+    m, d = spec.models[k], spec.d_dists[k]
+    model = pkg.Model(m, d, THR, context=ctx)
+    scene = pkg.Scene(spec.scene, d, 5, context=ctx)
+    model.ppf_lookup(scene)
+    mine = _lookup_state(model)
+    assert mine["codes"].size > 30_000_000
+    mc, sc = (m.points, m.normals), (spec.scene.points, spec.scene.normals)
+    post = ref_gpu.post(mc, sc, d, mine["codes"], mine["counts"])
+    _compare_lookup(mine, post, mine["codes"], mine["counts"])
+    _record("bench_model3_post", n_kept=int(mine["codes"].size), reference_post_ms=post["elapsed_ms"],
+            engine_post_ms=mine["stats"]["total_ms"] - mine["stats"]["vote_ms"])
 
 
 @pytest.mark.parametrize("k", range(4))
