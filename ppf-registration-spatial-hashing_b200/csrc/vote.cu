@@ -332,12 +332,21 @@ __device__ __forceinline__ void vote_item(const VoteArgs& a, uint32_t slot_of_it
         // and the model angle beta_m in its low 21.  With y = (beta_s + 2^20 -
         // beta_m) << 11, i.e. alpha + pi in 2^-32 turns (the row bits and the
         // exact-only flag shift out), the bin is the high word of y * 30 and
-        // the low word is the position inside the bin.
+        // the low word the position inside the bin; a vote is ambiguous when
+        // that position is within the margin m = 6 units of an edge.  One
+        // 32 x 32 -> 64 multiply gives both words of the margin-shifted angle
+        // y' = y - m:  30 y' = 30 y - 30 m, so a vote is unambiguous exactly
+        // when the low word of 30 y' is at most m_span, and its high word is
+        // then the bin of y.  For the ambiguous votes the high word is still
+        // in [0, 29] (y' wraps to 2^32 + y - m only when 30 y < 30 m, giving
+        // 29), so their provisional fast cell stays inside the accumulator.
         constexpr int kShift = 32 - PPF_ANGLE_BITS;
-        const uint32_t bsh = (bw + (1u << (PPF_ANGLE_BITS - 1))) << kShift;
-        constexpr uint32_t m_lo = (PPF_BIN_MARGIN_UNITS * PPF_N_ANGLE) << kShift;
+        const uint32_t bsh = ((bw + (1u << (PPF_ANGLE_BITS - 1))) << kShift) -
+                             ((uint32_t)PPF_BIN_MARGIN_UNITS << kShift);
         constexpr uint32_t m_span =
             ((1u << PPF_ANGLE_BITS) - 2 * PPF_BIN_MARGIN_UNITS * PPF_N_ANGLE) << kShift;
+        // (bin, position) of a margin-shifted angle: high and low word of 30 y'
+        auto bin_pos = [](uint32_t yp) { return (unsigned long long)yp * (uint32_t)PPF_N_ANGLE; };
         const uint32_t* ep = a.entries + start + lane;
         const uint32_t n_here = end - start;
         // A vote near a bin edge was counted in its fast cell; move it to the
@@ -347,10 +356,10 @@ __device__ __forceinline__ void vote_item(const VoteArgs& a, uint32_t slot_of_it
           for (int u = 0; u < kUnroll; ++u) {
             const uint32_t pos = (uint32_t)(first_entry + 32 * u - a.entries);
             const uint32_t e = __ldg(a.entries + pos);
-            const uint32_t y = bsh - (e << kShift);
-            if (!(y * (uint32_t)PPF_N_ANGLE - m_lo > m_span)) continue;
+            const unsigned long long bp = bin_pos(bsh - (e << kShift));
+            if (!((uint32_t)bp > m_span)) continue;
             const uint32_t row = (e >> PPF_ANGLE_BITS) * kBins;
-            const uint32_t fast = row + __umulhi(y, (uint32_t)PPF_N_ANGLE);
+            const uint32_t fast = row + (uint32_t)(bp >> 32);
             const uint32_t exact = row + exact_bin<kCheck>(a, pos, vv);
             if (exact != fast && in_range<kCheck>(a, 7, exact, cells)) {
               atomicAdd(&acc[fast], 0xffffffffu);
@@ -379,9 +388,9 @@ __device__ __forceinline__ void vote_item(const VoteArgs& a, uint32_t slot_of_it
             for (int u = 0; u < kUnroll; ++u) c[u] = __ldg(ep + 32 * u);
 #pragma unroll
             for (int u = 0; u < kUnroll; ++u) {
-              const uint32_t y = bsh - (c[u] << kShift);
-              amb |= y * (uint32_t)PPF_N_ANGLE - m_lo > m_span;
-              c[u] = (c[u] >> PPF_ANGLE_BITS) * kBins + __umulhi(y, (uint32_t)PPF_N_ANGLE);
+              const unsigned long long bp = bin_pos(bsh - (c[u] << kShift));
+              amb |= (uint32_t)bp > m_span;
+              c[u] = (c[u] >> PPF_ANGLE_BITS) * kBins + (uint32_t)(bp >> 32);
             }
 #pragma unroll
             for (int u = 0; u < kUnroll; ++u)
@@ -390,9 +399,9 @@ __device__ __forceinline__ void vote_item(const VoteArgs& a, uint32_t slot_of_it
           }
           for (uint32_t k = nfull * 32 * kUnroll + lane; k < n_here; k += 32) {
             const uint32_t e = __ldg(a.entries + start + k);
-            const uint32_t y = bsh - (e << kShift);
-            uint32_t cell = (e >> PPF_ANGLE_BITS) * kBins + __umulhi(y, (uint32_t)PPF_N_ANGLE);
-            if (y * (uint32_t)PPF_N_ANGLE - m_lo > m_span) {
+            const unsigned long long bp = bin_pos(bsh - (e << kShift));
+            uint32_t cell = (e >> PPF_ANGLE_BITS) * kBins + (uint32_t)(bp >> 32);
+            if ((uint32_t)bp > m_span) {
               cell = (e >> PPF_ANGLE_BITS) * kBins + exact_bin<kCheck>(a, start + k, vv);
               ++st.exact;
             }
