@@ -59,6 +59,57 @@ THR = 0.3
 # re-read by concurrent work items while still in L2, so its DRAM bytes scale
 # with its votes; the 3047-point model's tables fit L2 entirely.
 DRAM_BYTES_PER_VOTE = (0.04995, 0.03125, 0.04418, 0.001337)
+# Shared-memory bank wavefronts per warp-wide atomic of the vote kernel, from
+# ncu on the first model's profile case
+# (l1tex__data_pipe_lsu_wavefronts_mem_shared_op_atom.sum over
+# smsp__inst_executed_op_shared_atom.sum).
+VOTE_WAVEFRONTS_PER_ATOMIC = 1.90
+
+
+def shared_atomic_peaks(device):
+    """Warp-wide shared atomics one SM completes per cycle, measured by the
+    probe library (peaks/shared_atomic_peak.cu) for its three address
+    patterns: one wavefront, two wavefronts, and one word for all lanes.
+    Best of three launches each; None when the probe is not built."""
+    import ctypes
+
+    lib_path = ROOT / "ppf-registration-spatial-hashing_b200" / "libppf_peaks.so"
+    if not lib_path.exists():
+        return None
+    lib = ctypes.CDLL(str(lib_path))
+    f = lib.ppf_peak_shared_atomics
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double),
+                  ctypes.POINTER(ctypes.c_double)]
+    out = {}
+    for pattern, name in ((0, "1_wavefront"), (1, "2_wavefronts"), (2, "one_word")):
+        best = 0.0
+        for _ in range(3):
+            rate, ms = ctypes.c_double(), ctypes.c_double()
+            rc = f(device, pattern, 20000, ctypes.byref(rate), ctypes.byref(ms))
+            if rc != 0:
+                raise RuntimeError(f"shared atomic probe failed: CUDA error {rc}")
+            best = max(best, rate.value)
+        out[name] = best
+    return out
+
+
+def atomic_roofline(peaks, votes, vote_s, sm_mhz, n_sm):
+    """The vote kernel's warp-wide shared atomics per SM-cycle against the
+    probe's rate.  Every vote is one lane of a warp-wide atomic; the unrolled
+    passes keep all 32 lanes busy and the masked remainder of a segment holds
+    about 1% of the votes, so the kernel issues about votes / 32 of them.  The
+    ceiling at the kernel's own conflict level interpolates the probe's cycles
+    per atomic linearly between one and two wavefronts."""
+    if not peaks or vote_s <= 0 or not sm_mhz:
+        return None
+    achieved = votes / 32.0 / (vote_s * sm_mhz * 1e6 * n_sm)
+    c1, c2 = 1.0 / peaks["1_wavefront"], 1.0 / peaks["2_wavefronts"]
+    ceiling = 1.0 / (c1 + (VOTE_WAVEFRONTS_PER_ATOMIC - 1.0) * (c2 - c1))
+    return {"unit": "warp-wide shared atomics per SM cycle", "achieved": achieved,
+            "peak_measured": peaks, "wavefronts_per_atomic": VOTE_WAVEFRONTS_PER_ATOMIC,
+            "ceiling_at_kernel_conflicts": ceiling, "frac": achieved / ceiling,
+            "frac_of_conflict_free": achieved / peaks["1_wavefront"], "sm_mhz": sm_mhz, "sms": n_sm}
 
 
 def dist_env():
@@ -646,6 +697,9 @@ def main():
             dist.destroy_process_group()
         return
     peak, peak_kind = measured_peaks()
+    clocks = clk.summary()
+    atomics = atomic_roofline(shared_atomic_peaks(local), votes, vote_ms / 1000.0, clocks.get("sm_mhz"),
+                              torch.cuda.get_device_properties(dev).multi_processor_count)
     alg_bytes = 4.0 * votes + 32.0 * pairs
     vote_s = vote_ms / 1000.0
     achieved = alg_bytes / vote_s / 1e9 if vote_s > 0 else 0.0
@@ -675,16 +729,18 @@ def main():
                      "traffic": traffic / args.steps,
                      "traffic_note": "DRAM bytes per launch: measured bytes per vote of each model's profile "
                                      "case times its votes; the entries are served from L2 (about 2% of the "
-                                     "algorithmic bytes reach DRAM), and the kernel is limited by shared-memory "
-                                     "atomic wavefronts (l1tex 75% of peak on the profile case)",
+                                     "algorithmic bytes reach DRAM); the kernel is latency-bound on its L2 entry "
+                                     "loads, with the l1tex data pipe (shared atomics + loads) at 63% of peak on the "
+                                     "profile case",
                      "alg_bytes_per_launch": alg_bytes / args.steps,
                      "alg_bytes_rule": "4 B per vote + 32 B per scene pair evaluated (pairs x vote chunks of the model)",
                      "vote_chunks": chunks,
-                     "vote_ms_per_launch": vote_ms / args.steps},
+                     "vote_ms_per_launch": vote_ms / args.steps,
+                     "shared_atomics": atomics},
         "gpu_launches": int(launches),
         "vote_segments_tuned": [int(s["vote_segment"]) for s in stats[0]],
         "recall": recall,
-        "clocks": clk.summary(),
+        "clocks": clocks,
     }
     if e2e:
         line["e2e"] = e2e

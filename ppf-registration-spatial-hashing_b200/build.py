@@ -18,6 +18,9 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 BUILD = ROOT / "_build" / "ppf_b200"
 LIB = PKG / "libppf_b200.so"
+# measurement probe used by bench.py (not part of the engine's C ABI)
+PEAKS_SRC = PKG / "peaks" / "shared_atomic_peak.cu"
+PEAKS_LIB = PKG / "libppf_peaks.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [
@@ -76,6 +79,9 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     if jobs or force or not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
         cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs)]
         run(cmd)
+    if force or _needs(PEAKS_LIB, PEAKS_SRC, []):
+        run([nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", str(PEAKS_SRC), "-o",
+             str(PEAKS_LIB)])
     return LIB
 
 
