@@ -174,6 +174,10 @@ __device__ __forceinline__ uint32_t exact_bin(const VoteArgs& a, uint32_t pos, f
 // Per-block shared state of a vote kernel besides the dynamic queue and
 // accumulator.
 struct VoteShared {
+  // the item's scene reference point, its normal and rows 1-2 of its frame:
+  // read from here by the scene walk of each tile, so that they do not hold
+  // 14 registers through the vote passes between walks
+  float4 p_r, n_r, f_r1, f_r2;
   uint32_t item, next, max, base;
   uint32_t scan_seg[kVoteWarps];   // scratch of the per-tile segment scan
   uint32_t scan_emit[kVoteWarps];  // scratch of the emission scan
@@ -239,12 +243,17 @@ __device__ __forceinline__ void vote_item(const VoteArgs& a, uint32_t slot_of_it
     const uint32_t ref = (uint32_t)(((unsigned long long)(item / a.n_chunks) * a.perm_mul) % a.n_ref);
     const uint32_t sr = ref * a.ref_df;
     const uint32_t mr_lo = c * a.chunk;
-    // every thread derives the frame of s_r itself (a broadcast load and a
-    // few dozen flops per item), so no lane-divergent code precedes a barrier
-    const float4 p4 = a.s_pts[sr], n4 = a.s_nrm[sr];
-    const float3 pr = make_float3(p4.x, p4.y, p4.z);
-    const float3 nr = make_float3(n4.x, n4.y, n4.z);
-    const FrameYZ fs = frame_yz(pr, nr);
+    // thread 0 publishes the frame of s_r; the barrier after the clear makes
+    // it visible, and the previous item's readers are past the item-fetch
+    // barrier before it is overwritten
+    if (tid == 0) {
+      const float4 p4 = a.s_pts[sr], n4 = a.s_nrm[sr];
+      const FrameYZ f = frame_yz(make_float3(p4.x, p4.y, p4.z), make_float3(n4.x, n4.y, n4.z));
+      sh.p_r = p4;
+      sh.n_r = n4;
+      sh.f_r1 = f.r1;
+      sh.f_r2 = f.r2;
+    }
     for (uint32_t i = tid; i < cells; i += kVoteThreads) acc[i] = 0u;
     block_sync();
 
@@ -256,7 +265,9 @@ __device__ __forceinline__ void vote_item(const VoteArgs& a, uint32_t slot_of_it
       if (i < a.n_s && i != sr) {
         float4 pi4 = a.s_pts[i], ni4 = a.s_nrm[i];
         float3 pi = make_float3(pi4.x, pi4.y, pi4.z);
-        float4 f = pair_feature(pr, nr, pi, make_float3(ni4.x, ni4.y, ni4.z), a.d_dist);
+        const float4 p4 = sh.p_r, n4 = sh.n_r;
+        float4 f = pair_feature(make_float3(p4.x, p4.y, p4.z), make_float3(n4.x, n4.y, n4.z), pi,
+                                make_float3(ni4.x, ni4.y, ni4.z), a.d_dist);
         uint32_t key = feature_key(f);
         if (key != 0u) {
           uint32_t run = ht_lookup(a.ht_keys, a.ht_runs, a.ht_mask, key);
@@ -270,6 +281,9 @@ __device__ __forceinline__ void vote_item(const VoteArgs& a, uint32_t slot_of_it
               st.matched += 1;
             }
             if (len) {
+              FrameYZ fs;
+              fs.r1 = sh.f_r1;
+              fs.r2 = sh.f_r2;
               v = frame_point_yz(fs, pi);
               bool degenerate = fabsf(v.x) + fabsf(v.y) < 1e-12f || !isfinite(v.x) || !isfinite(v.y);
               beta = angle21(v) | ((degenerate || __ldg(a.run_flags + run)) ? kExactOnly : 0u);
@@ -349,15 +363,24 @@ __device__ __forceinline__ void vote_item(const VoteArgs& a, uint32_t slot_of_it
         auto bin_pos = [](uint32_t yp) { return (unsigned long long)yp * (uint32_t)PPF_N_ANGLE; };
         const uint32_t* ep = a.entries + start + lane;
         const uint32_t n_here = end - start;
-        // A vote near a bin edge was counted in its fast cell; move it to the
-        // cell of the reference's exact arithmetic (rare: ~1.7e-4 of votes).
-        auto fix_up = [&](const uint32_t* first_entry) {
-#pragma unroll 1
-          for (int u = 0; u < kUnroll; ++u) {
-            const uint32_t pos = (uint32_t)(first_entry + 32 * u - a.entries);
-            const uint32_t e = __ldg(a.entries + pos);
+        // Votes near a bin edge were counted in their fast cell; move them to
+        // the cell of the reference's exact arithmetic (rare: ~1.7e-4 of
+        // votes).  The pass's entries are still in registers (c), so only the
+        // exact path's own loads remain; pass_pos is the position of this
+        // lane's first entry of the pass.
+        auto fix_up = [&](uint32_t pass_pos, const uint32_t(&c)[kUnroll]) {
+          uint32_t mask = 0;
+#pragma unroll
+          for (int u = 0; u < kUnroll; ++u)
+            if ((uint32_t)bin_pos(bsh - (c[u] << kShift)) > m_span) mask |= 1u << u;
+          while (mask) {
+            const int u = __ffs(mask) - 1;
+            mask &= mask - 1;
+            uint32_t e = c[0];
+#pragma unroll
+            for (int k = 1; k < kUnroll; ++k) e = (u == k) ? c[k] : e;
+            const uint32_t pos = pass_pos + 32u * (uint32_t)u;
             const unsigned long long bp = bin_pos(bsh - (e << kShift));
-            if (!((uint32_t)bp > m_span)) continue;
             const uint32_t row = (e >> PPF_ANGLE_BITS) * kBins;
             const uint32_t fast = row + (uint32_t)(bp >> 32);
             const uint32_t exact = row + exact_bin<kCheck>(a, pos, vv);
@@ -390,12 +413,10 @@ __device__ __forceinline__ void vote_item(const VoteArgs& a, uint32_t slot_of_it
             for (int u = 0; u < kUnroll; ++u) {
               const unsigned long long bp = bin_pos(bsh - (c[u] << kShift));
               amb |= (uint32_t)bp > m_span;
-              c[u] = (c[u] >> PPF_ANGLE_BITS) * kBins + (uint32_t)(bp >> 32);
+              const uint32_t cell = (c[u] >> PPF_ANGLE_BITS) * kBins + (uint32_t)(bp >> 32);
+              if (in_range<kCheck>(a, 8, cell, cells)) atomicAdd(&acc[cell], 1u);
             }
-#pragma unroll
-            for (int u = 0; u < kUnroll; ++u)
-              if (in_range<kCheck>(a, 8, c[u], cells)) atomicAdd(&acc[c[u]], 1u);
-            if (amb) fix_up(ep);
+            if (amb) fix_up(start + it * 32u * kUnroll + lane, c);
           }
           for (uint32_t k = nfull * 32 * kUnroll + lane; k < n_here; k += 32) {
             const uint32_t e = __ldg(a.entries + start + k);
