@@ -26,6 +26,10 @@ roofline: the vote kernel (dominant), algorithmic bytes 4 B per vote
         evaluated, over its CUDA-event time, against MEASURED_PEAKS.json.
 cpu_baseline: the CPU oracle (C++/OpenMP restatement of the reference path)
         on a bounded sample of scene reference points, scaled.
+served: (1 GPU) the small library preset of --serve on its first 24 requests:
+        plain ppf_registration per request, one batched lookup, and the request
+        loop under Poisson arrivals (p50/p99 latency), with the served poses
+        compared to plain; host wall clock, after the timed region.
 
 Multi-GPU: replicas (each rank registers its own copy of the scene; no
 collective on the data path), weak scaling; time = max over ranks.
@@ -465,7 +469,7 @@ def run_serve(args):
                                  "and 150% of the batched rate"}}
     if nominal:
         line["served_at_50_requests_per_s"] = nominal
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_large(args):
@@ -577,6 +581,10 @@ def main():
     ap.add_argument("--serve-scenes", type=int, default=0, help="scenes (requests); 0: the preset's")
     ap.add_argument("--serve-workers", type=int, default=0, help="request-loop workers; 0: the preset's")
     ap.add_argument("--serve-max-batch", type=int, default=16)
+    ap.add_argument("--no-serve", action="store_true",
+                    help="leave the served-mode summary out of the default bench line")
+    ap.add_argument("--bench-serve-scenes", type=int, default=24,
+                    help="requests of the served-mode summary in the default bench line (small library preset)")
     ap.add_argument("--profile-case", action="store_true",
                     help="one lookup of one model at ref_point_df=50 (short vote launch for ncu)")
     ap.add_argument("--profile-model", type=int, default=0)
@@ -591,7 +599,8 @@ def main():
     if args.profile_case or args.profile_all:
         return run_profile_case(args)
     if args.serve:
-        return run_serve(args)
+        print(json.dumps(run_serve(args)), flush=True)
+        return
     if args.large:
         return run_large(args)
 
@@ -746,6 +755,13 @@ def main():
         line["e2e"] = e2e
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(spec, sample_refs=args.cpu_refs)
+    if world == 1 and not args.no_serve:
+        # plain / batched / served on the small library preset, after the
+        # timed region (host wall clock; see run_serve)
+        sv = argparse.Namespace(**vars(args))
+        sv.serve_preset, sv.serve_scenes, sv.serve_workers = "small", args.bench_serve_scenes, 0
+        line["served"] = {k: v for k, v in run_serve(sv).items()
+                          if k not in ("mode", "metric", "unit", "higher_is_better", "n_gpus", "data", "dtype")}
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
