@@ -67,7 +67,7 @@ DRAM_BYTES_PER_VOTE = (0.04995, 0.03125, 0.04418, 0.001337)
 # ncu on the first model's profile case
 # (l1tex__data_pipe_lsu_wavefronts_mem_shared_op_atom.sum over
 # smsp__inst_executed_op_shared_atom.sum).
-VOTE_WAVEFRONTS_PER_ATOMIC = 1.90
+VOTE_WAVEFRONTS_PER_ATOMIC = 1.94
 
 
 def shared_atomic_peaks(device):
@@ -739,7 +739,7 @@ def main():
                      "traffic_note": "DRAM bytes per launch: measured bytes per vote of each model's profile "
                                      "case times its votes; the entries are served from L2 (about 2% of the "
                                      "algorithmic bytes reach DRAM); the kernel is latency-bound on its L2 entry "
-                                     "loads, with the l1tex data pipe (shared atomics + loads) at 63% of peak on the "
+                                     "loads, with the l1tex data pipe (shared atomics + loads) at 69% of peak on the "
                                      "profile case",
                      "alg_bytes_per_launch": alg_bytes / args.steps,
                      "alg_bytes_rule": "4 B per vote + 32 B per scene pair evaluated (pairs x vote chunks of the model)",
