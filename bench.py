@@ -326,7 +326,8 @@ def run_reference_arm(args):
 def run_cpu_config1(args):
     """BASELINE config 1 (2000-point model, 10000-point scene, ref_point_df 5,
     tau_d 0.05) registered in full by the CPU oracle on all host cores, and a
-    1-core run over every 10th scene reference point, projected."""
+    1-core run over every 10th scene reference point, projected (with
+    --cpu-one-core-full: the 1-core run registers in full as well)."""
     orc = ge.load_oracle()
     O = orc.Oracle()
     pkg = ge.load_package()
@@ -336,18 +337,24 @@ def run_cpu_config1(args):
     t0 = time.perf_counter()
     r = O.register((m.points, m.normals), (s.points, s.normals), d, 5, 0.3, n_threads=threads)
     full = time.perf_counter() - t0
+    line = {"mode": "cpu_config1", "workload": "config 1: 2000-pt superellipsoid, 10000-pt scene, "
+            "ref_point_df 5, tau_d 0.05, threshold 0.3, GPU-style clustering",
+            "n_votes": r["n_votes"], "all_cores": threads, "all_cores_s": full,
+            "all_cores_registrations_per_s": 1.0 / full}
     t0 = time.perf_counter()
-    r1 = O.register((m.points, m.normals), (s.points, s.normals), d, 5, 0.3, n_threads=1, sr_step=50)
-    one = time.perf_counter() - t0
-    n_ref = (len(s) + 4) // 5
-    one_proj = r1["t_build"] + r1["t_vote"] / max(r1["n_refs"], 1) * n_ref
-    print(json.dumps({"mode": "cpu_config1", "workload": "config 1: 2000-pt superellipsoid, 10000-pt scene, "
-                      "ref_point_df 5, tau_d 0.05, threshold 0.3, GPU-style clustering",
-                      "n_votes": r["n_votes"], "all_cores": threads, "all_cores_s": full,
-                      "all_cores_registrations_per_s": 1.0 / full,
-                      "one_core_sample_s": one, "one_core_sample_refs": r1["n_refs"],
-                      "one_core_projected_s": one_proj, "one_core_registrations_per_s_projected": 1.0 / one_proj}),
-          flush=True)
+    if args.cpu_one_core_full:
+        r1 = O.register((m.points, m.normals), (s.points, s.normals), d, 5, 0.3, n_threads=1)
+        one = time.perf_counter() - t0
+        line.update({"one_core_s": one, "one_core_registrations_per_s": 1.0 / one,
+                     "one_core_pose_equals_all_cores": bool(np.array_equal(r1["pose"], r["pose"]))})
+    else:
+        r1 = O.register((m.points, m.normals), (s.points, s.normals), d, 5, 0.3, n_threads=1, sr_step=50)
+        one = time.perf_counter() - t0
+        n_ref = (len(s) + 4) // 5
+        one_proj = r1["t_build"] + r1["t_vote"] / max(r1["n_refs"], 1) * n_ref
+        line.update({"one_core_sample_s": one, "one_core_sample_refs": r1["n_refs"],
+                     "one_core_projected_s": one_proj, "one_core_registrations_per_s_projected": 1.0 / one_proj})
+    print(json.dumps(line), flush=True)
 
 
 SERVE_PRESETS = {
@@ -566,6 +573,8 @@ def main():
     ap.add_argument("--avg", action="store_true", help="use_averaged_clusters on")
     ap.add_argument("--cpu-refs", type=int, default=2,
                     help="scene reference points per model in each CPU sample step")
+    ap.add_argument("--cpu-one-core-full", action="store_true",
+                    help="with --cpu-config1: register config 1 in full on one core too (minutes)")
     ap.add_argument("--cpu-config1", action="store_true",
                     help="config 1 registered in full by the CPU oracle (all cores) and a projected 1-core run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
