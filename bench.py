@@ -769,8 +769,11 @@ def main():
         # timed region (host wall clock; see run_serve)
         sv = argparse.Namespace(**vars(args))
         sv.serve_preset, sv.serve_scenes, sv.serve_workers = "small", args.bench_serve_scenes, 0
-        line["served"] = {k: v for k, v in run_serve(sv).items()
-                          if k not in ("mode", "metric", "unit", "higher_is_better", "n_gpus", "data", "dtype")}
+        try:
+            line["served"] = {k: v for k, v in run_serve(sv).items()
+                              if k not in ("mode", "metric", "unit", "higher_is_better", "n_gpus", "data", "dtype")}
+        except Exception as e:  # the summary is an addition; its failure must not cost the bench line
+            line["served"] = {"error": f"{type(e).__name__}: {e}"}
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
