@@ -746,7 +746,7 @@ def main():
                      "kernel": "vote_batch_kernel (one launch per step: the four lookups' vote passes)",
                      "traffic": traffic / args.steps,
                      "traffic_note": "DRAM bytes per launch: measured bytes per vote of each model's profile "
-                                     "case times its votes; the entries are served from L2 (about 2% of the "
+                                     "case times its votes; the entries are served from L2 (about 0.5% of the "
                                      "algorithmic bytes reach DRAM); the kernel is latency-bound on its L2 entry "
                                      "loads, with the l1tex data pipe (shared atomics + loads) at 69% of peak on the "
                                      "profile case",
